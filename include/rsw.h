@@ -1,0 +1,226 @@
+/*
+ * rsw.h -- C ABI of the B200 split-step wavefront propagation engine.
+ *
+ * Plain C types only (pointers, sizes, doubles); CUDA streams are passed as
+ * `void*` (a cudaStream_t, NULL = the legacy default stream). Every entry point
+ * returns an rsw_status and never exits the process; the message of the last
+ * failure on the calling thread is available from rsw_last_error().
+ *
+ * Field buffers are device memory owned by the caller, interleaved complex
+ * (complex128 = {double re, im}, complex64 = {float re, im}), contiguous,
+ * sample i at x = (i - N/2) * dx. Calls are asynchronous on the given stream
+ * unless stated otherwise. A plan or simulation object may be used by one host
+ * thread at a time.
+ *
+ * Semantics follow the reference's FP64 implementation (rave-sim big-wave):
+ * grating mask coordinates (big-wave/optical_element.py:341-377), the frequency
+ * cutoff index range (big-wave/propagation.py:74-97), the Fresnel transfer
+ * function (big-wave/propagation.py:124-128) and np.histogram detector binning
+ * (big-wave/propagation.py:279-320).
+ */
+#ifndef RSW_H
+#define RSW_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSW_ABI_VERSION 1
+
+typedef enum {
+    RSW_OK = 0,
+    RSW_ERR_INVALID = 1,      /* bad argument, size or configuration            */
+    RSW_ERR_UNSUPPORTED = 2,  /* valid but not implemented (e.g. N not 2^k)     */
+    RSW_ERR_CUDA = 3,         /* CUDA runtime error (message has the details)   */
+    RSW_ERR_NOMEM = 4,        /* device or host allocation failed               */
+    RSW_ERR_TIMEOUT = 5       /* a bounded device wait expired                  */
+} rsw_status;
+
+typedef enum {
+    RSW_C128 = 0,       /* complex128 field, all arithmetic FP64 ("c16")                  */
+    RSW_C64 = 1,        /* complex64 field, FP32 FFT, FP64 phases and intensity ("c8")    */
+} rsw_dtype;
+
+typedef struct rsw_plan_s *rsw_plan;
+typedef struct rsw_sim_s *rsw_sim;
+
+/* ---------------------------------------------------------------- errors */
+const char *rsw_last_error(void);
+int rsw_abi_version(void);
+/* Number of kernels this library launched since load (all threads). */
+uint64_t rsw_launch_count(void);
+/* sizeof of the ABI structs, for bindings to verify their layouts:
+ * 0 rsw_element, 1 rsw_sim_desc, 2 rsw_source, 3 rsw_source_run. */
+size_t rsw_struct_size(int which);
+
+/* Photon wavelength in metres for an energy in eV, evaluated exactly as the
+ * reference's convert_energy_wavelength (big-wave/propagation.py:26-28, :69-71). */
+double rsw_energy_to_wavelength(double energy_ev);
+
+/* ------------------------------------------------------------ FFT plans
+ * Replaces fast-wave's FFT<S> (fast-wave/src/fft.hpp:9-24, src/fft.cpp:6-48):
+ * a 1-D complex FFT of length N (a power of two, 16 <= N <= 2^26 for C64 and
+ * 2^24 for C128 in this version), forward unnormalised, inverse scaled by 1/N
+ * (the reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length.
+ * The plan owns its twiddle tables and scratch; it is bound to the device that
+ * is current at creation. */
+rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype);
+rsw_status rsw_plan_destroy(rsw_plan plan);
+rsw_status rsw_plan_info(rsw_plan plan, int64_t *n, int *dtype, int *log_rows,
+                         int *log_cols, int64_t *scratch_bytes);
+
+/* fast-wave FFT<S>::forward / inverse (src/fft.cpp:28-44); natural order in and
+ * out; in == out allowed. */
+rsw_status rsw_fft_forward(rsw_plan plan, const void *d_in, void *d_out, void *stream);
+rsw_status rsw_fft_inverse(rsw_plan plan, const void *d_in, void *d_out, void *stream);
+
+/* big-wave propagation.propagate (big-wave/propagation.py:100-138) and
+ * fast-wave propagate<S> (fast-wave/src/simulation.cpp:34-40): u <- iFFT(H * FFT(u))
+ * with H the Fresnel transfer function of distance dz and the big-wave frequency
+ * cutoff; on return d_U holds FFT(u_new) in natural order (the reference's
+ * postcondition). With skip_fft != 0, d_U must hold FFT(u) on entry and d_u is
+ * only written. d_U may be NULL when skip_fft == 0: then the spectrum is not
+ * stored (faster). */
+rsw_status rsw_propagate(rsw_plan plan, void *d_u, void *d_U, double dx, double wl,
+                         double dz, double cutoff_freq, int skip_fft, void *stream);
+
+/* ------------------------------------------------------- transmission
+ * The reference's per-element kernels (fast-wave/fwcuda/wrappers.hpp:9-39) with
+ * big-wave's discrete semantics. x of sample i is built per chunk of
+ * `chunk_size` samples exactly as big-wave's np.linspace does
+ * (optical_element.py:352-354); chunk_size <= 0 means one chunk.
+ * factor_a/factor_b are {re, im} pairs (the material factors of one sub-step). */
+rsw_status rsw_apply_grating_factors(rsw_plan plan, void *d_u, double dx, int64_t chunk_size,
+                                     double pitch, double dc, double x_position,
+                                     const double factor_a[2], const double factor_b[2],
+                                     void *stream);
+rsw_status rsw_apply_dba_grating_factors(rsw_plan plan, void *d_u, double dx,
+                                         int64_t chunk_size, double pitch0, double pitch1,
+                                         double dc0, double dc1, double x_position,
+                                         const double factor_a[2], const double factor_b[2],
+                                         void *stream);
+/* One z-row of a pixelised sample (big-wave/optical_element.py:432-476):
+ * u *= exp(i 2 pi dz / wl * interp(x, row_x, row_db, left=0, right=0)).
+ * h_row_db: host array of x_len {re, im} pairs (delta, beta) of the row. */
+rsw_status rsw_apply_sample_row(rsw_plan plan, void *d_u, double dx, double wl, double dz,
+                                double pixel_size_x, double x_position, int64_t x_len,
+                                const double *h_row_db, void *stream);
+/* u *= factor (fast-wave scale kernel, fwcuda/kernels.cu:160-172). */
+rsw_status rsw_scale(rsw_plan plan, void *d_u, const double factor[2], void *stream);
+/* Point-source field exp(-2 pi i r / wl)/sqrt(r) (big-wave/propagation.py:141-151). */
+rsw_status rsw_point_source(rsw_plan plan, void *d_u, double dx, double wl, double z,
+                            double x_source, void *stream);
+
+/* --------------------------------------------------------- detection
+ * square_and_downsample (big-wave/propagation.py:279-320): |u|^2 binned with
+ * np.histogram semantics into n_pix = int(detector_size // pixel_size_x) pixels,
+ * then scaled by cos(atan(x/z)) * dx * pixel_size_y / sqrt(x^2 + z^2).
+ * d_out: device array of n_pix doubles. Returns n_pix through *n_pix_out when
+ * non-NULL (d_out may then be NULL to query the size only). */
+rsw_status rsw_square_and_downsample(rsw_plan plan, const void *d_u, double dx,
+                                     double detector_size, double pixel_size_x,
+                                     double pixel_size_y, double z, double *d_out,
+                                     int64_t *n_pix_out, void *stream);
+
+/* Host-only helper (no GPU needed): the detector geometry used by
+ * rsw_square_and_downsample. bounds[j]..bounds[j+1] is the sample-index range
+ * binned into pixel j (np.histogram semantics), cosv/rv the per-pixel
+ * cos(atan(x/z)) and sqrt(x^2+z^2). Call with bounds == NULL to get n_pix. */
+rsw_status rsw_detector_geometry(int64_t n, double dx, double detector_size,
+                                 double pixel_size_x, double z, int64_t *n_pix,
+                                 int64_t *bounds, double *cosv, double *rv);
+
+/* ---------------------------------------------------------- simulations
+ * A whole per-source schedule (big-wave/wavesim.py:84-298, fast-wave
+ * run_simulation_inner, src/simulation.cpp:375-549) run on the fused engine:
+ * two HBM sweeps per split step, phase steps restarted from an in-HBM snapshot,
+ * detector output accumulated in FP64 on the device.
+ *
+ * Elements are given as a flat description (rsw_element). Energy-dependent
+ * inputs (wavelength, deltabeta values) are given per run. */
+typedef enum { RSW_EL_GRATING = 0, RSW_EL_DBA_GRATING = 1, RSW_EL_SAMPLE = 2 } rsw_element_type;
+
+typedef struct {
+    int type;                    /* rsw_element_type                                   */
+    double z_start;
+    double thickness;            /* grating: height of the structure (no substrate)    */
+    double substrate_thickness;
+    int nr_steps;                /* grating sub-steps                                  */
+    double pitch, pitch1;        /* grating pitch; DBA: pitch0, pitch1                 */
+    double dc[2], dc1[2];        /* duty cycle (start, end); DBA: dc0, dc1             */
+    int n_x_positions;
+    const double *x_positions;   /* phase-step shifts (host memory, copied)           */
+    /* sample */
+    double pixel_size_x, pixel_size_z;
+    int64_t grid_z, grid_x;      /* grid shape [z_len, x_len]                           */
+    const int8_t *grid;          /* host int8 material indices (copied), 0 = vacuum    */
+    int n_materials;             /* materials 1..n_materials                           */
+} rsw_element;
+
+typedef struct {
+    int64_t n;
+    int dtype;                   /* rsw_dtype */
+    double dx;
+    double z_detector;
+    double detector_size;
+    double pixel_size_x, pixel_size_y;
+    int64_t chunk_size;          /* big-wave chunk_size (grating coordinates)            */
+    int n_elements;
+    const rsw_element *elements;
+    const double *cutoff_angles; /* n_elements + 1                                       */
+} rsw_sim_desc;
+
+typedef enum { RSW_SRC_PLANE = 0, RSW_SRC_POINT = 1, RSW_SRC_VECTOR = 2 } rsw_source_type;
+
+typedef struct {
+    int type;                    /* rsw_source_type                                       */
+    double x, z;                 /* point: position; plane/vector: z of the input field  */
+    const void *h_field;         /* vector: host field (N complex of the sim dtype)       */
+    const void *d_field;         /* vector: or a device field                             */
+} rsw_source;
+
+typedef struct {
+    double energy_ev;            /* photon energy; wavelength = h c / (E e)               */
+    /* deltabeta of every material as {delta, beta}, per element:
+     * gratings: [a, b, substrate] (zeros for absent materials);
+     * samples: [material 1 .. n_materials]. Concatenated in element order. */
+    const double *deltabeta;
+    int64_t n_deltabeta;         /* number of {delta, beta} pairs                       */
+    double weight;               /* accumulation weight of this source's detector output */
+} rsw_source_run;
+
+rsw_status rsw_sim_create(rsw_sim *out, const rsw_sim_desc *desc);
+rsw_status rsw_sim_destroy(rsw_sim sim);
+/* Shape of the detector output: nr_phase_steps x n_pix. */
+rsw_status rsw_sim_shape(rsw_sim sim, int64_t *nr_phase_steps, int64_t *n_pix,
+                         int64_t *split_steps_per_source);
+/* Run one source and add weight * detected[phase][pix] to the device
+ * accumulator. Asynchronous on `stream`. */
+rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run *run,
+                       void *stream);
+/* Zero the accumulator. */
+rsw_status rsw_sim_reset(rsw_sim sim, void *stream);
+/* Copy the accumulator (nr_phase_steps * n_pix doubles) to host memory;
+ * synchronises `stream`. */
+rsw_status rsw_sim_read(rsw_sim sim, double *h_out, void *stream);
+/* Device pointer of the accumulator (for peers / collectives). */
+rsw_status rsw_sim_accumulator(rsw_sim sim, double **d_acc);
+/* Copy the final field of the last phase step of the last run (natural order,
+ * N complex of the sim dtype) to device memory. */
+rsw_status rsw_sim_final_field(rsw_sim sim, void *d_dst, void *stream);
+
+/* Per-kernel-kind device timing of the next rsw_sim_run calls (CUDA events on
+ * the run's stream). kind: 0 = row pass, 1 = column pass, 2 = detection.
+ * rsw_sim_timing returns the summed milliseconds and launch counts since
+ * enabling; it synchronises. */
+rsw_status rsw_sim_set_timing(rsw_sim sim, int enable);
+rsw_status rsw_sim_timing(rsw_sim sim, int kind, double *ms, int64_t *launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSW_H */

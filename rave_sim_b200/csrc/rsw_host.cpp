@@ -1,0 +1,1223 @@
+// Host side of the rsw engine: FFT plans, the numpy-exact host arithmetic of
+// the reference's discrete decisions, the per-source schedule of
+// big-wave/wavesim.py:84-298 on the fused two-pass engine, and the C ABI
+// declared in include/rsw.h.
+//
+// Compiled with -ffp-contract=off: every scalar below is evaluated with the
+// reference's operation order and one rounding per operation.
+#include "rsw.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "rsw_internal.h"
+
+namespace rsw {
+cudaError_t launch_row_pass(const PassArgs &a, bool dbl, cudaStream_t s);
+cudaError_t launch_col_pass(const PassArgs &a, bool dbl, cudaStream_t s);
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
+                                   cudaStream_t s);
+cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
+                                   cudaStream_t s);
+cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cudaStream_t s);
+cudaError_t launch_copy(const void *in, void *out, int64_t n, bool dbl, cudaStream_t s);
+cudaError_t launch_point_source(void *u, int64_t n, double dx, double w, double z, double x_src, bool dbl,
+                                cudaStream_t s);
+cudaError_t launch_detect(const void *u, const int64_t *bounds, const double *cosv, const double *rv,
+                          int64_t n_pix, double dx, double psy, double *out, double *acc, double *comp,
+                          double weight, bool dbl, cudaStream_t s);
+cudaError_t launch_zero(double *p, int64_t n, cudaStream_t s);
+cudaError_t launch_fill_ones(void *u, int64_t n, bool dbl, cudaStream_t s);
+unsigned long long launch_count();
+}  // namespace rsw
+
+using namespace rsw;
+using cplx = std::complex<double>;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string t_last_error;
+
+static rsw_status fail(rsw_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return st;
+}
+
+#define CU(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(e_ == cudaErrorMemoryAllocation ? RSW_ERR_NOMEM : RSW_ERR_CUDA,        \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+#define CHECK(expr)                   \
+    do {                              \
+        rsw_status s_ = (expr);       \
+        if (s_ != RSW_OK) return s_;  \
+    } while (0)
+
+// -------------------------------------------------- reference host arithmetic
+// big-wave/propagation.py:26-28, :69-71. The constants are evaluated the way
+// the reference writes them (mantissa * 10 ** exponent, one rounding each):
+// 1.602176634 * 10**-19 is one ulp away from the literal 1.602176634e-19, and
+// at phases of 1e10 rad one ulp of the wavelength is 1e-6 rad.
+static double wavelength(double energy_ev) {
+    const double h_planck = 6.62607004 * std::pow(10.0, -34.0);
+    const double c_0 = 299792458.0;
+    const double ev_to_joule = 1.602176634 * std::pow(10.0, -19.0);
+    return h_planck * c_0 / (energy_ev * ev_to_joule);
+}
+
+// Python float floor division `a // b` (CPython float_floor_div semantics).
+static double py_floordiv(double a, double b) {
+    double mod = std::fmod(a, b);
+    double div = (a - mod) / b;
+    if (mod != 0.0) {
+        if ((b < 0) != (mod < 0)) div -= 1.0;
+    }
+    double fl;
+    if (div != 0.0) {
+        fl = std::floor(div);
+        if (div - fl > 0.5) fl += 1.0;
+    } else {
+        fl = std::copysign(0.0, a / b);
+    }
+    return fl;
+}
+
+// material_factor(db, t, wl) = np.exp(2j*pi*t/wl * db) (big-wave/optical_element.py:36-39)
+static cplx material_factor(double delta, double beta, double t, double wl) {
+    const double y = (2.0 * M_PI * t) / wl;
+    const double re = -(y * beta);
+    const double im = y * delta;
+    const double e = std::exp(re);
+    return cplx(e * std::cos(im), e * std::sin(im));
+}
+
+// Propagator scalars of propagate() (big-wave/propagation.py:74-137).
+static PropArgs make_prop(int64_t n, double dx, double wl, double dz, double cutoff_freq, bool apply_h) {
+    PropArgs p{};
+    p.has_h = apply_h ? 1 : 0;
+    p.c = (M_PI * wl) * dz;
+    const double phi = ((-2.0 * M_PI) / wl) * dz;
+    p.A = make_double2(std::cos(phi), std::sin(phi));
+    p.fac = 1.0 / double(n);
+    p.dx = dx;
+    const double frac = cutoff_freq * dx;
+    const double start = std::ceil(double(n) * frac);
+    if (!(start > double(n) / 2.0)) {
+        p.has_cut = 1;
+        p.cut_lo = int64_t(start);
+        p.cut_hi = std::min<int64_t>(n - int64_t(start) + 1, n);
+    }
+    return p;
+}
+
+// np.linspace chunk coordinates of generate_grating_chunk
+// (big-wave/optical_element.py:341-357): per chunk (x_start, step).
+static void chunk_coords(int64_t n, int64_t cs, double dx, double x_pos, std::vector<double> &xs,
+                         std::vector<double> &st) {
+    xs.clear();
+    st.clear();
+    if (cs <= 0 || cs > n) cs = n;
+    for (int64_t idx = 0; idx < n; idx += cs) {
+        const int64_t cnt = std::min(cs, n - idx);
+        const int64_t start = idx - n / 2;
+        const double x_start = double(start) * dx + x_pos;
+        const double x_stop = x_start + double(cnt) * dx;
+        const double delta = x_stop - x_start;
+        xs.push_back(x_start);
+        st.push_back(delta / double(cnt));
+    }
+}
+
+// Detector geometry of square_and_downsample (big-wave/propagation.py:279-320):
+// np.histogram bin membership turned into sample-index boundaries (positions
+// (i - N/2)*dx are monotone in i), plus per-pixel cos(atan(x/z)) and r.
+struct DetectorGeom {
+    int64_t n_pix = 0;
+    std::vector<int64_t> bounds;  // n_pix + 1
+    std::vector<double> cosv, rv;
+};
+
+static rsw_status detector_geom(int64_t n, double dx, double det_size, double psx, double z, DetectorGeom &g) {
+    if (!(psx > 0) || !(det_size > 0)) return fail(RSW_ERR_INVALID, "detector size and pixel size must be positive");
+    const double nf = py_floordiv(det_size, psx);
+    const int64_t outsize = int64_t(nf);
+    if (outsize > n) return fail(RSW_ERR_INVALID, "detector has %lld pixels > N", (long long)outsize);
+    g.n_pix = outsize;
+    const double first = -(double(outsize) / 2.0) * psx;
+    const double last = (double(outsize) / 2.0 + 1.0) * psx;
+    const int64_t nb = outsize + 1;
+    const double denom = last - first;
+    const double step = denom / double(nb);
+    auto edge = [&](int64_t i) { return i >= nb ? last : double(i) * step + first; };
+    auto pos = [&](int64_t i) { return (double(i) - double(n / 2)) * dx; };
+    auto bin = [&](double a) -> int64_t {
+        const double f = ((a - first) / denom) * double(nb);
+        int64_t idx = int64_t(f);
+        if (idx == nb) idx -= 1;
+        if (a < edge(idx)) idx -= 1;
+        if (a >= edge(idx + 1) && idx != nb - 1) idx += 1;
+        return idx;
+    };
+    // kept samples: first <= a <= last
+    int64_t lo = 0, hi = n;  // first i with pos(i) >= first
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (pos(mid) >= first) hi = mid; else lo = mid + 1;
+    }
+    const int64_t n_lo = lo;
+    lo = 0;
+    hi = n;  // first i with pos(i) > last
+    while (lo < hi) {
+        int64_t mid = lo + (hi - lo) / 2;
+        if (pos(mid) > last) hi = mid; else lo = mid + 1;
+    }
+    const int64_t n_end = std::max(lo, n_lo);
+    g.bounds.assign(outsize + 1, n_end);
+    for (int64_t j = 0; j <= outsize; ++j) {
+        int64_t a = n_lo, b = n_end;  // first i in [n_lo, n_end) with bin(pos(i)) >= j
+        while (a < b) {
+            int64_t mid = a + (b - a) / 2;
+            if (bin(pos(mid)) >= j) b = mid; else a = mid + 1;
+        }
+        g.bounds[j] = a;
+    }
+    // x = (np.arange(n) - n // 2) * psx with n the float detector_size // psx (util.py:78-82)
+    const double half = py_floordiv(nf, 2.0);
+    g.cosv.resize(outsize);
+    g.rv.resize(outsize);
+    for (int64_t j = 0; j < outsize; ++j) {
+        const double x = (double(j) - half) * psx;
+        g.cosv[j] = std::cos(std::atan(x / z));
+        g.rv[j] = std::sqrt(x * x + z * z);
+    }
+    return RSW_OK;
+}
+
+// ---------------------------------------------------------------- buffers
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    rsw_status alloc(size_t b) {
+        if (bytes >= b && p) return RSW_OK;
+        release();
+        if (b == 0) return RSW_OK;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cudaGetLastError();
+            return fail(RSW_ERR_NOMEM, "cudaMalloc(%zu): %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return RSW_OK;
+    }
+    template <typename T> rsw_status upload(const std::vector<T> &v) {
+        CHECK(alloc(v.size() * sizeof(T)));
+        if (!v.empty()) CU(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        return RSW_OK;
+    }
+};
+
+// -------------------------------------------------------------------- plan
+static constexpr int ROW_MAX_C128 = 13, COL_MAX_C128 = 11;
+static constexpr int ROW_MAX_C64 = 14, COL_MAX_C64 = 12;
+static std::atomic<uint64_t> g_api_calls{0};
+
+struct rsw_plan_s {
+    int64_t n = 0;
+    int log_n = 0;
+    int dtype = RSW_C128;
+    int log_n1 = 0, log_n2 = 0;  // column level, row level
+    int device = 0;
+    DevBuf tw_row, tw_col, tw4_lo, tw4_hi, tw4_hi_inv;
+    int tw4_shift = 0;
+    DevBuf scratch;                                       // N samples, for the natural-order APIs
+    DevBuf det_bounds, det_cos, det_r;                    // cached detector geometry
+    double det_key[5] = {0, 0, 0, 0, 0};
+    int64_t det_npix = -1;
+    DevBuf chunk_xs, chunk_st;                            // per-call chunk tables
+    DevBuf sample_grid, sample_db, sample_fac;            // per-call sample row data
+    bool dbl() const { return dtype == RSW_C128; }
+    size_t elem() const { return dbl() ? 16 : 8; }
+};
+
+// W_M^m = exp(-2 pi i m / M), accurate to < 1 ulp (long double evaluation)
+static cplx twiddle(int64_t m, int64_t M) {
+    m %= M;
+    if (m < 0) m += M;
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)M;
+    return cplx(double(cosl(ang)), double(sinl(ang)));
+}
+
+template <typename T> static void push_c(std::vector<T> &v, cplx c) {
+    v.push_back(T(c.real()));
+    v.push_back(T(c.imag()));
+}
+
+// Block twiddle table of a block of length 2^log_l (layout of Radix<LOG_L>::twoff).
+template <typename T> static std::vector<T> block_twiddles(int log_l) {
+    std::vector<T> v;
+    if (log_l < 4) return v;
+    const int ns = (log_l + 3) / 4;
+    const int lr0 = log_l - 4 * (ns - 1);
+    for (int s = 0; s < ns - 1; ++s) {
+        const int lr = s == 0 ? lr0 : 4;
+        const int ls = log_l - lr0 - 4 * s;
+        const int64_t R = int64_t(1) << lr, S = int64_t(1) << ls;
+        for (int64_t q = 1; q < R; ++q)
+            for (int64_t j = 0; j < S; ++j) push_c(v, twiddle(j * q, R * S));
+    }
+    if (v.empty()) push_c(v, cplx(1, 0));
+    return v;
+}
+
+template <typename T> static rsw_status plan_tables(rsw_plan_s *p) {
+    CHECK(p->tw_row.upload(block_twiddles<T>(p->log_n2)));
+    if (p->log_n1 > 0) {
+        CHECK(p->tw_col.upload(block_twiddles<T>(p->log_n1)));
+        const int h = (p->log_n + 1) / 2;
+        p->tw4_shift = h;
+        std::vector<T> lo, hi, hinv;
+        for (int64_t a = 0; a < (int64_t(1) << h); ++a) push_c(lo, twiddle(a, p->n));
+        const double inv_n = 1.0 / double(p->n);
+        for (int64_t b = 0; b < (int64_t(1) << (p->log_n - h)); ++b) {
+            const cplx w = twiddle(b << h, p->n);
+            push_c(hi, w);
+            push_c(hinv, std::conj(w) * inv_n);
+        }
+        CHECK(p->tw4_lo.upload(lo));
+        CHECK(p->tw4_hi.upload(hi));
+        CHECK(p->tw4_hi_inv.upload(hinv));
+    }
+    return RSW_OK;
+}
+
+static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *l2) {
+    if (n < 16 || (n & (n - 1)) != 0)
+        return fail(RSW_ERR_UNSUPPORTED, "N = %lld: this version supports powers of two >= 16", (long long)n);
+    int lg = 0;
+    while ((int64_t(1) << lg) < n) ++lg;
+    const int row_max = dtype == RSW_C128 ? ROW_MAX_C128 : ROW_MAX_C64;
+    const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
+    if (lg <= row_max) {
+        *l1 = 0;
+        *l2 = lg;
+    } else {
+        int a = std::min(col_max, lg / 2);
+        int b = lg - a;
+        if (b > row_max) {
+            a = lg - row_max;
+            b = row_max;
+        }
+        if (a > col_max || a < 4)
+            return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the two-level limit 2^%d for this dtype", lg,
+                        row_max + col_max);
+        *l1 = a;
+        *l2 = b;
+    }
+    *log_n = lg;
+    return RSW_OK;
+}
+
+static PassArgs base_args(const rsw_plan_s *p) {
+    PassArgs a{};
+    a.n = p->n;
+    a.log_n1 = p->log_n1;
+    a.log_n2 = p->log_n2;
+    a.tw_row = p->tw_row.p;
+    a.tw_col = p->tw_col.p;
+    a.tw4_lo = p->tw4_lo.p;
+    a.tw4_hi = p->tw4_hi.p;
+    a.tw4_hi_inv = p->tw4_hi_inv.p;
+    a.tw4_shift = p->tw4_shift;
+    a.pr.fac = 1.0 / double(p->n);
+    a.tr.kind = TR_NONE;
+    return a;
+}
+
+// ------------------------------------------------------------ timing hooks
+struct TimingLog {
+    bool enabled = false;
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double ms[3] = {0, 0, 0};
+    int64_t launches[3] = {0, 0, 0};
+    cudaEvent_t get() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int kind, cudaStream_t s, Rec &r) {
+        r.kind = kind;
+        r.a = get();
+        r.b = get();
+        cudaEventRecord(r.a, s);
+    }
+    void end(Rec &r, cudaStream_t s) {
+        cudaEventRecord(r.b, s);
+        recs.push_back(r);
+    }
+    void collect() {
+        for (auto &r : recs) {
+            cudaEventSynchronize(r.b);
+            float t = 0;
+            cudaEventElapsedTime(&t, r.a, r.b);
+            ms[r.kind] += t;
+            launches[r.kind] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        recs.clear();
+    }
+    ~TimingLog() {
+        for (auto &r : recs) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+static rsw_status run_row(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s, TimingLog *tl = nullptr) {
+    TimingLog::Rec r{};
+    if (tl && tl->enabled) tl->begin(0, s, r);
+    cudaError_t e = launch_row_pass(a, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "row pass (2^%d): %s", a.log_n2, cudaGetErrorString(e));
+    if (tl && tl->enabled) tl->end(r, s);
+    return RSW_OK;
+}
+static rsw_status run_col(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s, TimingLog *tl = nullptr) {
+    TimingLog::Rec r{};
+    if (tl && tl->enabled) tl->begin(1, s, r);
+    cudaError_t e = launch_col_pass(a, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "column pass (2^%d): %s", a.log_n1, cudaGetErrorString(e));
+    if (tl && tl->enabled) tl->end(r, s);
+    return RSW_OK;
+}
+
+// ================================================================== C ABI
+extern "C" {
+
+const char *rsw_last_error(void) { return t_last_error.c_str(); }
+int rsw_abi_version(void) { return RSW_ABI_VERSION; }
+uint64_t rsw_launch_count(void) { return uint64_t(launch_count()); }
+double rsw_energy_to_wavelength(double energy_ev) { return wavelength(energy_ev); }
+size_t rsw_struct_size(int which) {
+    switch (which) {
+    case 0: return sizeof(rsw_element);
+    case 1: return sizeof(rsw_sim_desc);
+    case 2: return sizeof(rsw_source);
+    case 3: return sizeof(rsw_source_run);
+    default: return 0;
+    }
+}
+
+rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
+    if (!out) return fail(RSW_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
+    int lg, l1, l2;
+    CHECK(plan_split(n, dtype, &lg, &l1, &l2));
+    std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
+    if (!p) return fail(RSW_ERR_NOMEM, "host allocation failed");
+    p->n = n;
+    p->log_n = lg;
+    p->dtype = dtype;
+    p->log_n1 = l1;
+    p->log_n2 = l2;
+    CU(cudaGetDevice(&p->device));
+    CHECK(p->dbl() ? plan_tables<double>(p.get()) : plan_tables<float>(p.get()));
+    *out = p.release();
+    return RSW_OK;
+}
+
+rsw_status rsw_plan_destroy(rsw_plan plan) {
+    delete plan;
+    return RSW_OK;
+}
+
+rsw_status rsw_plan_info(rsw_plan p, int64_t *n, int *dtype, int *log_rows, int *log_cols, int64_t *scratch) {
+    if (!p) return fail(RSW_ERR_INVALID, "plan is NULL");
+    if (n) *n = p->n;
+    if (dtype) *dtype = p->dtype;
+    if (log_rows) *log_rows = p->log_n1;
+    if (log_cols) *log_cols = p->log_n2;
+    if (scratch) *scratch = int64_t(p->scratch.bytes);
+    return RSW_OK;
+}
+
+static rsw_status need_scratch(rsw_plan_s *p) { return p->scratch.alloc(size_t(p->n) * p->elem()); }
+
+rsw_status rsw_fft_forward(rsw_plan p, const void *in, void *out, void *stream) {
+    if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    CHECK(need_scratch(p));
+    PassArgs a = base_args(p);
+    if (p->log_n1 > 0) {
+        a.in = in;
+        a.out = p->scratch.p;
+        a.flags = PF_FWD | PF_TW;
+        CHECK(run_col(p, a, s));
+        a.in = p->scratch.p;
+    } else {
+        a.in = in;
+        a.out = p->scratch.p;
+    }
+    a.out = p->scratch.p;
+    a.flags = PF_FWD;
+    CHECK(run_row(p, a, s));
+    cudaError_t e = launch_spec_to_natural(p->scratch.p, out, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_fft_inverse(rsw_plan p, const void *in, void *out, void *stream) {
+    if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    CHECK(need_scratch(p));
+    cudaError_t e = launch_natural_to_spec(in, p->scratch.p, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+    PassArgs a = base_args(p);
+    a.in = p->scratch.p;
+    if (p->log_n1 > 0) {
+        a.out = p->scratch.p;
+        a.flags = PF_SPEC_IN | PF_INV | PF_TW;
+        CHECK(run_row(p, a, s));
+        a.in = p->scratch.p;
+        a.out = out;
+        a.flags = PF_INV;
+        CHECK(run_col(p, a, s));
+    } else {
+        a.out = out;
+        a.flags = PF_SPEC_IN | PF_INV | PF_SCALE;
+        CHECK(run_row(p, a, s));
+    }
+    return RSW_OK;
+}
+
+rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, double dz, double cutoff_freq,
+                         int skip_fft, void *stream) {
+    if (!p || !u) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (skip_fft && !U) return fail(RSW_ERR_INVALID, "skip_fft needs the spectrum U");
+    if (!(dx > 0) || !(wl > 0)) return fail(RSW_ERR_INVALID, "dx and wl must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a = base_args(p);
+    a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0);
+    const bool two = p->log_n1 > 0;
+    // 1. spectrum of u in the internal layout, in place in u
+    if (skip_fft) {
+        cudaError_t e = launch_natural_to_spec(U, u, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+    } else if (two) {
+        a.in = u;
+        a.out = u;
+        a.flags = PF_FWD | PF_TW;
+        CHECK(run_col(p, a, s));
+    }
+    a.in = u;
+    a.out = u;
+    if (U) {
+        // 2a. forward row level + transfer function, spectrum out; copy to U in natural order
+        a.flags = skip_fft ? PF_SPEC_IN : PF_FWD;
+        CHECK(run_row(p, a, s));
+        cudaError_t e = launch_spec_to_natural(u, U, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+        a.pr.has_h = 0;
+        a.pr.has_cut = 0;
+        a.flags = PF_SPEC_IN | PF_INV | (two ? PF_TW : PF_SCALE);
+        CHECK(run_row(p, a, s));
+    } else {
+        a.flags = (skip_fft ? PF_SPEC_IN : PF_FWD) | PF_INV | (two ? PF_TW : PF_SCALE);
+        CHECK(run_row(p, a, s));
+    }
+    if (two) {
+        a.pr = PropArgs{};
+        a.flags = PF_INV;
+        CHECK(run_col(p, a, s));
+    }
+    return RSW_OK;
+}
+
+static rsw_status grating_trans(rsw_plan_s *p, TransArgs &tr, int64_t chunk_size, double dx, double x_pos,
+                                cudaStream_t stream) {
+    std::vector<double> xs, st;
+    chunk_coords(p->n, chunk_size, dx, x_pos, xs, st);
+    for (double v : st)
+        if (v == 0.0) return fail(RSW_ERR_UNSUPPORTED, "grating coordinate step underflows to zero");
+    tr.half_n_floor = p->n / 2;
+    if (xs.size() == 1) {
+        tr.chunk_size = 0;
+        tr.xstart0 = xs[0];
+        tr.step0 = st[0];
+    } else {
+        tr.chunk_size = chunk_size;
+        // the plan's chunk tables may still be read by earlier work on this stream
+        CU(cudaStreamSynchronize(stream));
+        CHECK(p->chunk_xs.upload(xs));
+        CHECK(p->chunk_st.upload(st));
+        tr.chunk_xstart = (const double *)p->chunk_xs.p;
+        tr.chunk_step = (const double *)p->chunk_st.p;
+    }
+    return RSW_OK;
+}
+
+rsw_status rsw_apply_grating_factors(rsw_plan p, void *u, double dx, int64_t chunk_size, double pitch, double dc,
+                                     double x_position, const double fa[2], const double fb[2], void *stream) {
+    if (!p || !u || !fa || !fb) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (!(pitch > 0)) return fail(RSW_ERR_INVALID, "pitch must be positive");
+    TransArgs tr{};
+    tr.kind = TR_GRATING;
+    tr.pitch0 = pitch;
+    tr.dc0 = dc;
+    tr.half_dc0 = dc / 2;
+    tr.fa = make_double2(fa[0], fa[1]);
+    tr.fb = make_double2(fb[0], fb[1]);
+    CHECK(grating_trans(p, tr, chunk_size, dx, x_position, (cudaStream_t)stream));
+    cudaError_t e = launch_trans(u, p->n, tr, p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "grating: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_apply_dba_grating_factors(rsw_plan p, void *u, double dx, int64_t chunk_size, double pitch0,
+                                         double pitch1, double dc0, double dc1, double x_position,
+                                         const double fa[2], const double fb[2], void *stream) {
+    if (!p || !u || !fa || !fb) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (!(pitch0 > 0) || !(pitch1 > 0)) return fail(RSW_ERR_INVALID, "pitches must be positive");
+    TransArgs tr{};
+    tr.kind = TR_DBA;
+    tr.pitch0 = pitch0;
+    tr.pitch1 = pitch1;
+    tr.dc0 = dc0;
+    tr.half_dc0 = dc0 / 2;
+    tr.dc1 = dc1;
+    tr.fa = make_double2(fa[0], fa[1]);
+    tr.fb = make_double2(fb[0], fb[1]);
+    CHECK(grating_trans(p, tr, chunk_size, dx, x_position, (cudaStream_t)stream));
+    cudaError_t e = launch_trans(u, p->n, tr, p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "dba grating: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+// Sample row: the row's deltabeta values are turned into a per-pixel material
+// table (each distinct value becomes one "material"), so the device code is
+// the same as for a grid row.
+static rsw_status sample_trans(rsw_plan_s *p, TransArgs &tr, double dx, double wl, double dz, double psx,
+                               double x_pos, int64_t x_len, const int8_t *grid_row_host,
+                               const std::vector<cplx> &mat_db /* [0] = vacuum */) {
+    if (x_len < 2) return fail(RSW_ERR_UNSUPPORTED, "sample rows need at least 2 pixels");
+    if (!(psx > 0)) return fail(RSW_ERR_INVALID, "pixel_size_x must be positive");
+    tr.kind = TR_SAMPLE;
+    tr.dx = dx;
+    tr.half_n = double(p->n) / 2.0;
+    tr.psx = psx;
+    tr.sample_xpos = x_pos;
+    tr.sample_hw = (double(x_len) * psx) * 0.5;
+    tr.sample_inv_psx = 1.0 / psx;
+    tr.x_len = x_len;
+    tr.sample_y = (2.0 * M_PI * dz) / wl;
+    std::vector<double> db, fac;
+    for (const cplx &d : mat_db) {
+        db.push_back(d.real());
+        db.push_back(d.imag());
+        const cplx f = material_factor(d.real(), d.imag(), dz, wl);
+        fac.push_back(f.real());
+        fac.push_back(f.imag());
+    }
+    CHECK(p->sample_db.upload(db));
+    CHECK(p->sample_fac.upload(fac));
+    CHECK(p->sample_grid.alloc(size_t(x_len)));
+    CU(cudaMemcpy(p->sample_grid.p, grid_row_host, size_t(x_len), cudaMemcpyHostToDevice));
+    tr.row_grid = (const int8_t *)p->sample_grid.p;
+    tr.mat_db = (const double2 *)p->sample_db.p;
+    tr.mat_factor = (const double2 *)p->sample_fac.p;
+    return RSW_OK;
+}
+
+rsw_status rsw_apply_sample_row(rsw_plan p, void *u, double dx, double wl, double dz, double psx, double x_pos,
+                                int64_t x_len, const double *h_row_db, void *stream) {
+    if (!p || !u || !h_row_db) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (x_len > 127 * 1024 * 1024) return fail(RSW_ERR_INVALID, "row too long");
+    // distinct values -> material indices (0 = vacuum)
+    std::vector<cplx> mats{cplx(0, 0)};
+    std::vector<int8_t> grid(size_t(std::max<int64_t>(x_len, 0)));
+    for (int64_t j = 0; j < x_len; ++j) {
+        const cplx d(h_row_db[2 * j], h_row_db[2 * j + 1]);
+        size_t m = 0;
+        while (m < mats.size() && !(mats[m] == d)) ++m;
+        if (m == mats.size()) {
+            if (mats.size() >= 127) return fail(RSW_ERR_UNSUPPORTED, "more than 126 distinct values in a row");
+            mats.push_back(d);
+        }
+        grid[j] = int8_t(m);
+    }
+    TransArgs tr{};
+    // the plan's row buffers may still be read by earlier work on this stream
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    CHECK(sample_trans(p, tr, dx, wl, dz, psx, x_pos, x_len, grid.data(), mats));
+    cudaError_t e = launch_trans(u, p->n, tr, p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "sample: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_scale(rsw_plan p, void *u, const double f[2], void *stream) {
+    if (!p || !u || !f) return fail(RSW_ERR_INVALID, "NULL argument");
+    TransArgs tr{};
+    tr.kind = TR_SCALAR;
+    tr.fa = make_double2(f[0], f[1]);
+    cudaError_t e = launch_trans(u, p->n, tr, p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "scale: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_point_source(rsw_plan p, void *u, double dx, double wl, double z, double x_src, void *stream) {
+    if (!p || !u) return fail(RSW_ERR_INVALID, "NULL argument");
+    const double w = (-2.0 * M_PI) / wl;
+    cudaError_t e = launch_point_source(u, p->n, dx, w, z, x_src, p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "point source: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+static rsw_status plan_detector(rsw_plan_s *p, double dx, double det, double psx, double z) {
+    const double key[5] = {dx, det, psx, z, double(p->n)};
+    if (p->det_npix >= 0 && std::memcmp(key, p->det_key, sizeof key) == 0) return RSW_OK;
+    DetectorGeom g;
+    CHECK(detector_geom(p->n, dx, det, psx, z, g));
+    CHECK(p->det_bounds.upload(g.bounds));
+    CHECK(p->det_cos.upload(g.cosv));
+    CHECK(p->det_r.upload(g.rv));
+    std::memcpy(p->det_key, key, sizeof key);
+    p->det_npix = g.n_pix;
+    return RSW_OK;
+}
+
+rsw_status rsw_square_and_downsample(rsw_plan p, const void *u, double dx, double det, double psx, double psy,
+                                     double z, double *out, int64_t *n_pix_out, void *stream) {
+    if (!p) return fail(RSW_ERR_INVALID, "plan is NULL");
+    CHECK(plan_detector(p, dx, det, psx, z));
+    if (n_pix_out) *n_pix_out = p->det_npix;
+    if (!out) return n_pix_out ? RSW_OK : fail(RSW_ERR_INVALID, "out is NULL");
+    if (!u) return fail(RSW_ERR_INVALID, "u is NULL");
+    cudaError_t e = launch_detect(u, (const int64_t *)p->det_bounds.p, (const double *)p->det_cos.p,
+                                  (const double *)p->det_r.p, p->det_npix, dx, psy, out, nullptr, nullptr, 0.0,
+                                  p->dbl(), (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "detect: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_detector_geometry(int64_t n, double dx, double det, double psx, double z, int64_t *n_pix,
+                                 int64_t *bounds, double *cosv, double *rv) {
+    if (!n_pix) return fail(RSW_ERR_INVALID, "n_pix is NULL");
+    if (n < 1) return fail(RSW_ERR_INVALID, "n must be positive");
+    DetectorGeom g;
+    CHECK(detector_geom(n, dx, det, psx, z, g));
+    *n_pix = g.n_pix;
+    if (bounds) std::copy(g.bounds.begin(), g.bounds.end(), bounds);
+    if (cosv) std::copy(g.cosv.begin(), g.cosv.end(), cosv);
+    if (rv) std::copy(g.rv.begin(), g.rv.end(), rv);
+    return RSW_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ simulations
+struct SimElement {
+    rsw_element d{};
+    std::vector<double> x_positions;
+    std::vector<int8_t> grid;
+    DevBuf grid_dev;
+    // grating chunk tables per phase-step position (when several chunks)
+    std::vector<std::unique_ptr<DevBuf>> chunk_xs, chunk_st;
+    std::vector<double> xs0, st0;  // single-chunk values per position
+    int64_t steps() const {
+        return d.type == RSW_EL_SAMPLE ? d.grid_z : int64_t(d.nr_steps) + (d.substrate_thickness > 0 ? 1 : 0);
+    }
+    double total_thickness() const {
+        return d.type == RSW_EL_SAMPLE ? d.pixel_size_z * double(d.grid_z) : d.thickness + d.substrate_thickness;
+    }
+};
+
+struct rsw_sim_s {
+    rsw_plan_s *plan = nullptr;
+    rsw_sim_desc d{};
+    std::vector<SimElement> els;
+    std::vector<double> cutoff_angles;
+    int64_t nr_phase_steps = 1;
+    int snap_el = -1;
+    DetectorGeom geom;
+    DevBuf bounds, cosv, rv;
+    DevBuf acc, comp;
+    DevBuf buf[2];
+    DevBuf mat_db, mat_fac;  // per-run sample material tables
+    int last_field = -1;
+    TimingLog tl;
+    int64_t split_steps = 0;
+    ~rsw_sim_s() { rsw_plan_destroy(plan); }
+};
+
+namespace {
+
+struct Runner {
+    rsw_sim_s *S;
+    rsw_plan_s *P;
+    cudaStream_t st;
+    double wl;
+    std::vector<double> cut;
+    // field state
+    int cur = 0;            // buffer index holding the field (or -1 when plane_pending)
+    bool mid = false;       // field in the row-pass ("mid") representation
+    bool ones = false;      // field is the plane wave u = 1, not yet materialised
+    int readonly = -1;      // buffer that must not be written (snapshot)
+    // per-run material factors: per element [fa? ...]
+    std::vector<std::vector<cplx>> db;  // deltabeta per element (gratings: a,b,sub; samples: materials 1..)
+
+    int target() const {
+        if (cur < 0) return readonly == 0 ? 1 : 0;
+        return cur == readonly ? 1 - cur : cur;
+    }
+
+    rsw_status split_step(const TransArgs &tr, double dz, double cutoff) {
+        const int dst = target();
+        PassArgs a = base_args(P);
+        a.tr = tr;
+        a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0);
+        if (P->log_n1 > 0) {
+            a.in = ones ? nullptr : S->buf[cur].p;
+            a.out = S->buf[dst].p;
+            a.flags = (mid ? PF_INV : 0) | PF_FWD | PF_TW | (tr.kind != TR_NONE ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
+            PropArgs keep = a.pr;
+            a.pr = PropArgs{};
+            CHECK(run_col(P, a, st, &S->tl));
+            a.pr = keep;
+            a.in = S->buf[dst].p;
+            a.tr.kind = TR_NONE;
+            a.flags = PF_FWD | PF_INV | PF_TW;
+            CHECK(run_row(P, a, st, &S->tl));
+            mid = true;
+        } else {
+            a.in = ones ? nullptr : S->buf[cur].p;
+            a.out = S->buf[dst].p;
+            a.flags = PF_FWD | PF_INV | PF_SCALE | (tr.kind != TR_NONE ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
+            CHECK(run_row(P, a, st, &S->tl));
+            mid = false;
+        }
+        cur = dst;
+        ones = false;
+        ++S->split_steps;
+        return RSW_OK;
+    }
+
+    rsw_status finalize() {
+        if (ones) {
+            const int dst = target();
+            cudaError_t e = launch_fill_ones(S->buf[dst].p, P->n, P->dbl(), st);
+            if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "fill: %s", cudaGetErrorString(e));
+            cur = dst;
+            ones = false;
+            mid = false;
+        }
+        if (mid) {
+            const int dst = target();
+            PassArgs a = base_args(P);
+            a.in = S->buf[cur].p;
+            a.out = S->buf[dst].p;
+            a.flags = PF_INV;
+            CHECK(run_col(P, a, st, &S->tl));
+            cur = dst;
+            mid = false;
+        }
+        return RSW_OK;
+    }
+
+    rsw_status detect(int64_t phase, double weight) {
+        TimingLog::Rec r{};
+        if (S->tl.enabled) S->tl.begin(2, st, r);
+        double *acc = (double *)S->acc.p + phase * S->geom.n_pix;
+        double *comp = (double *)S->comp.p + phase * S->geom.n_pix;
+        cudaError_t e = launch_detect(S->buf[cur].p, (const int64_t *)S->bounds.p, (const double *)S->cosv.p,
+                                      (const double *)S->rv.p, S->geom.n_pix, S->d.dx, S->d.pixel_size_y, nullptr,
+                                      acc, comp, weight, P->dbl(), st);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "detect: %s", cudaGetErrorString(e));
+        if (S->tl.enabled) S->tl.end(r, st);
+        return RSW_OK;
+    }
+
+    rsw_status apply(int ei, int64_t step, double cutoff) {
+        SimElement &el = S->els[ei];
+        const rsw_element &e = el.d;
+        const std::vector<cplx> &m = db[ei];
+        if (e.type == RSW_EL_GRATING || e.type == RSW_EL_DBA_GRATING) {
+            const double z_step = e.thickness / double(e.nr_steps);
+            const cplx fa = material_factor(m[0].real(), m[0].imag(), z_step, wl);
+            const cplx fb = material_factor(m[1].real(), m[1].imag(), z_step, wl);
+            for (int i = 0; i < e.nr_steps; ++i) {
+                const double zf = double(i) / double(e.nr_steps);
+                TransArgs tr{};
+                tr.kind = e.type == RSW_EL_GRATING ? TR_GRATING : TR_DBA;
+                tr.fa = make_double2(fa.real(), fa.imag());
+                tr.fb = make_double2(fb.real(), fb.imag());
+                tr.pitch0 = e.pitch;
+                tr.pitch1 = e.pitch1;
+                tr.dc0 = (1.0 - zf) * e.dc[0] + zf * e.dc[1];
+                tr.half_dc0 = tr.dc0 / 2;
+                tr.dc1 = (1.0 - zf) * e.dc1[0] + zf * e.dc1[1];
+                if (el.chunk_xs.empty()) {
+                    tr.chunk_size = 0;
+                    tr.xstart0 = el.xs0[step];
+                    tr.step0 = el.st0[step];
+                } else {
+                    tr.chunk_size = S->d.chunk_size;
+                    tr.chunk_xstart = (const double *)el.chunk_xs[step]->p;
+                    tr.chunk_step = (const double *)el.chunk_st[step]->p;
+                }
+                CHECK(split_step(tr, z_step, cutoff));
+            }
+            if (e.substrate_thickness > 0) {
+                const cplx fs = material_factor(m[2].real(), m[2].imag(), e.substrate_thickness, wl);
+                TransArgs tr{};
+                tr.kind = TR_SCALAR;
+                tr.fa = make_double2(fs.real(), fs.imag());
+                CHECK(split_step(tr, e.substrate_thickness, cutoff));
+            }
+            return RSW_OK;
+        }
+        // sample
+        const double psz = e.pixel_size_z;
+        TransArgs tr{};
+        tr.kind = TR_SAMPLE;
+        tr.dx = S->d.dx;
+        tr.half_n = double(P->n) / 2.0;
+        tr.psx = e.pixel_size_x;
+        tr.sample_xpos = el.x_positions[step];
+        tr.sample_hw = (double(e.grid_x) * e.pixel_size_x) * 0.5;
+        tr.sample_inv_psx = 1.0 / e.pixel_size_x;
+        tr.x_len = e.grid_x;
+        tr.sample_y = (2.0 * M_PI * psz) / wl;
+        const size_t off = size_t(ei) * 128;
+        tr.mat_db = (const double2 *)S->mat_db.p + off;
+        tr.mat_factor = (const double2 *)S->mat_fac.p + off;
+        for (int64_t r = 0; r < e.grid_z; ++r) {
+            tr.row_grid = (const int8_t *)el.grid_dev.p + r * e.grid_x;
+            CHECK(split_step(tr, psz, cutoff));
+        }
+        return RSW_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+rsw_status rsw_sim_create(rsw_sim *out, const rsw_sim_desc *desc) {
+    if (!out || !desc) return fail(RSW_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    if (desc->n_elements < 0 || (desc->n_elements > 0 && !desc->elements))
+        return fail(RSW_ERR_INVALID, "bad element list");
+    if (!desc->cutoff_angles) return fail(RSW_ERR_INVALID, "cutoff_angles is NULL");
+    if (!(desc->dx > 0)) return fail(RSW_ERR_INVALID, "dx must be positive");
+    std::unique_ptr<rsw_sim_s> S(new (std::nothrow) rsw_sim_s());
+    if (!S) return fail(RSW_ERR_NOMEM, "host allocation failed");
+    CHECK(rsw_plan_create(&S->plan, desc->n, desc->dtype));
+    S->d = *desc;
+    S->d.elements = nullptr;
+    S->cutoff_angles.assign(desc->cutoff_angles, desc->cutoff_angles + desc->n_elements + 1);
+    for (double a : S->cutoff_angles)
+        if (!(a >= 0 && a <= M_PI / 2 + 1e-12)) return fail(RSW_ERR_INVALID, "cutoff angles must be in [0, pi/2]");
+    const double z_tol = 1e-8;
+    double last_z = 0;
+    S->els.resize(desc->n_elements);
+    for (int i = 0; i < desc->n_elements; ++i) {
+        const rsw_element &e = desc->elements[i];
+        SimElement &el = S->els[i];
+        el.d = e;
+        if (e.n_x_positions < 1 || !e.x_positions) return fail(RSW_ERR_INVALID, "element %d: no x_positions", i);
+        el.x_positions.assign(e.x_positions, e.x_positions + e.n_x_positions);
+        el.d.x_positions = nullptr;
+        if (e.type == RSW_EL_GRATING || e.type == RSW_EL_DBA_GRATING) {
+            if (e.nr_steps < 1 || !(e.thickness > 0) || e.substrate_thickness < 0 || !(e.pitch > 0) ||
+                (e.type == RSW_EL_DBA_GRATING && !(e.pitch1 > 0)))
+                return fail(RSW_ERR_INVALID, "element %d: invalid grating", i);
+            const bool multi = desc->chunk_size > 0 && desc->chunk_size < desc->n;
+            for (double xp : el.x_positions) {
+                std::vector<double> xs, st;
+                chunk_coords(desc->n, desc->chunk_size, desc->dx, xp, xs, st);
+                for (double v : st)
+                    if (v == 0.0) return fail(RSW_ERR_UNSUPPORTED, "grating coordinate step underflows");
+                if (multi) {
+                    el.chunk_xs.emplace_back(new DevBuf());
+                    el.chunk_st.emplace_back(new DevBuf());
+                    CHECK(el.chunk_xs.back()->upload(xs));
+                    CHECK(el.chunk_st.back()->upload(st));
+                } else {
+                    el.xs0.push_back(xs[0]);
+                    el.st0.push_back(st[0]);
+                }
+            }
+        } else if (e.type == RSW_EL_SAMPLE) {
+            if (e.grid_z < 1 || e.grid_x < 2 || !e.grid || !(e.pixel_size_x > 0) || !(e.pixel_size_z > 0))
+                return fail(RSW_ERR_INVALID, "element %d: invalid sample", i);
+            if (e.n_materials < 0 || e.n_materials > 126) return fail(RSW_ERR_INVALID, "element %d: materials", i);
+            el.grid.assign(e.grid, e.grid + size_t(e.grid_z * e.grid_x));
+            for (int8_t g : el.grid)
+                if (g < 0 || g > e.n_materials) return fail(RSW_ERR_INVALID, "element %d: grid index %d", i, int(g));
+            el.d.grid = nullptr;
+            CHECK(el.grid_dev.alloc(el.grid.size()));
+            CU(cudaMemcpy(el.grid_dev.p, el.grid.data(), el.grid.size(), cudaMemcpyHostToDevice));
+        } else {
+            return fail(RSW_ERR_INVALID, "element %d: unknown type %d", i, e.type);
+        }
+        // check_validity (fast-wave/src/simulation.cpp:237-274)
+        if (e.z_start < last_z - z_tol) return fail(RSW_ERR_INVALID, "element %d starts before the previous ends", i);
+        last_z = e.z_start + el.total_thickness();
+        const int64_t k = e.n_x_positions;
+        if (k > 1) {
+            if (S->nr_phase_steps != 1 && S->nr_phase_steps != k)
+                return fail(RSW_ERR_INVALID, "inconsistent number of phase steps");
+            S->nr_phase_steps = k;
+            if (S->snap_el < 0) S->snap_el = i;
+        }
+    }
+    if (last_z > desc->z_detector + z_tol) return fail(RSW_ERR_INVALID, "detector before the last element");
+    CHECK(detector_geom(desc->n, desc->dx, desc->detector_size, desc->pixel_size_x, desc->z_detector, S->geom));
+    CHECK(S->bounds.upload(S->geom.bounds));
+    CHECK(S->cosv.upload(S->geom.cosv));
+    CHECK(S->rv.upload(S->geom.rv));
+    const size_t nacc = size_t(S->nr_phase_steps * S->geom.n_pix);
+    CHECK(S->acc.alloc(std::max<size_t>(nacc, 1) * sizeof(double)));
+    CHECK(S->comp.alloc(std::max<size_t>(nacc, 1) * sizeof(double)));
+    CU(cudaMemset(S->acc.p, 0, nacc * sizeof(double)));
+    CU(cudaMemset(S->comp.p, 0, nacc * sizeof(double)));
+    const size_t fb = size_t(desc->n) * S->plan->elem();
+    CHECK(S->buf[0].alloc(fb));
+    if (S->nr_phase_steps > 1) CHECK(S->buf[1].alloc(fb));
+    CHECK(S->mat_db.alloc(size_t(std::max(desc->n_elements, 1)) * 128 * sizeof(double2)));
+    CHECK(S->mat_fac.alloc(size_t(std::max(desc->n_elements, 1)) * 128 * sizeof(double2)));
+    *out = S.release();
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_destroy(rsw_sim s) {
+    delete s;
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_shape(rsw_sim S, int64_t *nps, int64_t *npix, int64_t *steps) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    if (nps) *nps = S->nr_phase_steps;
+    if (npix) *npix = S->geom.n_pix;
+    if (steps) *steps = S->split_steps;
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_reset(rsw_sim S, void *stream) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    const int64_t n = S->nr_phase_steps * S->geom.n_pix;
+    cudaError_t e = launch_zero((double *)S->acc.p, n, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = launch_zero((double *)S->comp.p, n, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reset: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_read(rsw_sim S, double *h, void *stream) {
+    if (!S || !h) return fail(RSW_ERR_INVALID, "NULL argument");
+    const size_t n = size_t(S->nr_phase_steps * S->geom.n_pix);
+    CU(cudaMemcpyAsync(h, S->acc.p, n * sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_accumulator(rsw_sim S, double **d) {
+    if (!S || !d) return fail(RSW_ERR_INVALID, "NULL argument");
+    *d = (double *)S->acc.p;
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_final_field(rsw_sim S, void *dst, void *stream) {
+    if (!S || !dst) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (S->last_field < 0) return fail(RSW_ERR_INVALID, "no run yet");
+    CU(cudaMemcpyAsync(dst, S->buf[S->last_field].p, size_t(S->d.n) * S->plan->elem(), cudaMemcpyDeviceToDevice,
+                       (cudaStream_t)stream));
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_set_timing(rsw_sim S, int enable) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    S->tl.collect();
+    S->tl.enabled = enable != 0;
+    for (int k = 0; k < 3; ++k) {
+        S->tl.ms[k] = 0;
+        S->tl.launches[k] = 0;
+    }
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_timing(rsw_sim S, int kind, double *ms, int64_t *launches) {
+    if (!S || kind < 0 || kind > 2) return fail(RSW_ERR_INVALID, "bad argument");
+    S->tl.collect();
+    if (ms) *ms = S->tl.ms[kind];
+    if (launches) *launches = S->tl.launches[kind];
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
+    if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (!(run->energy_ev > 0)) return fail(RSW_ERR_INVALID, "energy must be positive");
+    ++g_api_calls;
+    Runner R;
+    R.S = S;
+    R.P = S->plan;
+    R.st = (cudaStream_t)stream;
+    R.wl = wavelength(run->energy_ev);
+    for (double a : S->cutoff_angles) R.cut.push_back(std::sin(a) / R.wl);
+    // deltabeta per element
+    int64_t k = 0;
+    std::vector<double> dbh(size_t(std::max<int64_t>(S->d.n_elements, 1)) * 128 * 2, 0.0);
+    std::vector<double> fch(dbh.size(), 0.0);
+    R.db.resize(S->els.size());
+    for (size_t i = 0; i < S->els.size(); ++i) {
+        const rsw_element &e = S->els[i].d;
+        const int cnt = e.type == RSW_EL_SAMPLE ? e.n_materials : 3;
+        if (k + cnt > run->n_deltabeta || (cnt > 0 && !run->deltabeta))
+            return fail(RSW_ERR_INVALID, "deltabeta table too short (%lld values)", (long long)run->n_deltabeta);
+        for (int m = 0; m < cnt; ++m, ++k) R.db[i].push_back(cplx(run->deltabeta[2 * k], run->deltabeta[2 * k + 1]));
+        if (e.type == RSW_EL_SAMPLE) {
+            const double psz = e.pixel_size_z;
+            for (int m = 0; m < cnt; ++m) {
+                const cplx d = R.db[i][m];
+                const cplx f = material_factor(d.real(), d.imag(), psz, R.wl);
+                dbh[(i * 128 + m + 1) * 2] = d.real();
+                dbh[(i * 128 + m + 1) * 2 + 1] = d.imag();
+                fch[(i * 128 + m + 1) * 2] = f.real();
+                fch[(i * 128 + m + 1) * 2 + 1] = f.imag();
+            }
+            fch[(i * 128) * 2] = 1.0;
+        }
+    }
+    CU(cudaMemcpyAsync(S->mat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
+    CU(cudaMemcpyAsync(S->mat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
+
+    rsw_sim_s &s = *S;
+    const double z_tol = 1e-8;
+    const int nel = int(s.els.size());
+    // ---- source (big-wave/source.py:46-101)
+    double cutoff = R.cut[0];
+    double z = nel > 0 ? s.els[0].d.z_start : s.d.z_detector;
+    R.cur = 0;
+    R.readonly = -1;
+    R.mid = false;
+    R.ones = false;
+    if (src->type == RSW_SRC_POINT) {
+        CHECK(rsw_point_source(R.P, s.buf[0].p, s.d.dx, R.wl, z - src->z, src->x, stream));
+        CHECK(R.split_step(TransArgs{}, 0.0, cutoff));
+    } else if (src->type == RSW_SRC_PLANE || src->type == RSW_SRC_VECTOR) {
+        if (src->type == RSW_SRC_PLANE) {
+            R.ones = true;
+            R.cur = -1;
+        } else if (src->d_field) {
+            CU(cudaMemcpyAsync(s.buf[0].p, src->d_field, size_t(s.d.n) * R.P->elem(), cudaMemcpyDeviceToDevice, R.st));
+        } else if (src->h_field) {
+            CU(cudaMemcpyAsync(s.buf[0].p, src->h_field, size_t(s.d.n) * R.P->elem(), cudaMemcpyHostToDevice, R.st));
+        } else {
+            return fail(RSW_ERR_INVALID, "vector source without a field");
+        }
+        const double dz = z - src->z;
+        if (dz != 0.0) CHECK(R.split_step(TransArgs{}, dz, cutoff));
+    } else {
+        return fail(RSW_ERR_INVALID, "unknown source type %d", src->type);
+    }
+
+    // ---- element loop (big-wave/wavesim.py:159-219)
+    struct Snap {
+        double z;
+        int cur;
+        bool mid, ones;
+    } snap{0, -1, false, false};
+    for (int i = 0; i < nel; ++i) {
+        const rsw_element &e = s.els[i].d;
+        if (z < e.z_start) CHECK(R.split_step(TransArgs{}, e.z_start - z, cutoff));
+        z = e.z_start;
+        if (i == s.snap_el) {
+            snap = Snap{z, R.cur, R.mid, R.ones};
+            R.readonly = R.cur;
+        }
+        cutoff = R.cut[i + 1];
+        CHECK(R.apply(i, 0, cutoff));
+        z = e.z_start + s.els[i].total_thickness();
+    }
+    if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, cutoff));
+    CHECK(R.finalize());
+    CHECK(R.detect(0, run->weight));
+
+    // ---- remaining phase steps from the snapshot (big-wave/wavesim.py:238-296)
+    for (int64_t step = 1; step < s.nr_phase_steps; ++step) {
+        R.cur = snap.cur;
+        R.mid = snap.mid;
+        R.ones = snap.ones;
+        z = snap.z;
+        cutoff = R.cut[s.snap_el];
+        for (int i = s.snap_el; i < nel; ++i) {
+            const rsw_element &e = s.els[i].d;
+            if (z < e.z_start) CHECK(R.split_step(TransArgs{}, e.z_start - z, cutoff));
+            z = e.z_start;
+            cutoff = R.cut[i + 1];
+            CHECK(R.apply(i, e.n_x_positions > 1 ? step : 0, cutoff));
+            z = e.z_start + s.els[i].total_thickness();
+        }
+        if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, cutoff));
+        CHECK(R.finalize());
+        CHECK(R.detect(step, run->weight));
+    }
+    s.last_field = R.cur;
+    return RSW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// Internal structures shared by the host library (rsw_host.cpp) and the CUDA
+// kernels (rsw_kernels.cu). Not part of the public ABI.
+#pragma once
+
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace rsw {
+
+enum TransKind : int {
+    TR_NONE = 0,
+    TR_SCALAR = 1,   // u *= fa
+    TR_GRATING = 2,  // u *= mask ? fa : fb, mask = mod(x/p + dc/2, 1) < dc
+    TR_DBA = 3,      // mask = (mod(x/p0 + dc0/2,1) < dc0) & (mod(x/p1,1) < dc1)
+    TR_SAMPLE = 4,   // u *= exp(i y * interp(x, row_x, row_db, 0, 0))
+};
+
+// Transmission through one grating sub-step, a substrate, or one sample row.
+struct TransArgs {
+    int kind;
+    double2 fa, fb;  // material factors
+    // grating coordinates: per-chunk np.linspace (start, step)
+    double pitch0, pitch1, half_dc0, dc0, dc1;
+    int64_t chunk_size;  // >= N: single chunk
+    double xstart0, step0;               // single-chunk values
+    const double *chunk_xstart;          // per-chunk tables (device) when several chunks
+    const double *chunk_step;
+    int64_t half_n_floor;                // N // 2 (integer)
+    // sample row
+    double dx;                           // field sampling
+    double half_n;                       // N / 2 (float)
+    double psx, sample_xpos, sample_hw;  // row_x[j] = (j*psx + xpos) - hw
+    double sample_inv_psx;
+    int64_t x_len;
+    const int8_t *row_grid;              // grid row (device)
+    const double2 *mat_db;               // deltabeta per material index (device), [0] = vacuum
+    const double2 *mat_factor;           // exp(i y db) per material index (device)
+    double sample_y;                     // 2 pi dz / wl
+};
+
+// Fresnel propagator of one split step (applied in the row pass).
+struct PropArgs {
+    int has_h;          // multiply by the transfer function
+    int has_cut;        // zero the cutoff range
+    double c;           // fl(fl(pi*wl)*dz)
+    double2 A;          // exp(-i 2 pi dz / wl)
+    double fac;         // 1.0 / N
+    double dx;
+    int64_t cut_lo, cut_hi;  // zero natural frequency indices k in [cut_lo, cut_hi)
+};
+
+enum PassFlags : int {
+    PF_FWD = 1,       // run the forward transform of this level
+    PF_INV = 2,       // run the inverse transform of this level
+    PF_TW = 4,        // apply the four-step twiddle (column: after fwd; row: after inv, with 1/N)
+    PF_TRANS = 8,     // apply transmission (column: between inv and fwd; single-level row: before fwd)
+    PF_SCALE = 16,    // single-level row: multiply by 1/N after the inverse
+    PF_ONES = 32,     // input is the plane wave u = 1 (input buffer not read)
+    PF_SPEC_IN = 64,  // row: input is a spectrum (digit-reversed layout), start with the inverse
+};
+
+struct PassArgs {
+    const void *in;
+    void *out;
+    int64_t n;
+    int log_n1;  // column level (0: single level)
+    int log_n2;  // row level
+    int flags;
+    const void *tw_row;   // block twiddles of the row level
+    const void *tw_col;   // block twiddles of the column level
+    const void *tw4_lo;   // four-step twiddles: W_N^m = lo[m & mask] * hi[m >> shift]
+    const void *tw4_hi;
+    const void *tw4_hi_inv;  // conj(hi) / N
+    int tw4_shift;
+    TransArgs tr;
+    PropArgs pr;
+};
+
+}  // namespace rsw
