@@ -206,6 +206,8 @@ rsw_status rsw_sim_reset(rsw_sim sim, void *stream);
 /* Copy the accumulator (nr_phase_steps * n_pix doubles) to host memory;
  * synchronises `stream`. */
 rsw_status rsw_sim_read(rsw_sim sim, double *h_out, void *stream);
+/* Copy the accumulator to device memory (asynchronous on `stream`). */
+rsw_status rsw_sim_read_device(rsw_sim sim, double *d_out, void *stream);
 /* Device pointer of the accumulator (for peers / collectives). */
 rsw_status rsw_sim_accumulator(rsw_sim sim, double **d_acc);
 /* Copy the final field of the last phase step of the last run (natural order,

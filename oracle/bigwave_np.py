@@ -83,13 +83,27 @@ def transfer_function(n: int, dx: float, wl: float, dz: float) -> np.ndarray:
     return np.exp(-1j * 2 * np.pi / wl * dz) * np.exp(1j * np.pi * wl * dz * (fx**2))
 
 
-def propagate(u, U, sim: Sim, dz: float, cutoff_freq: float, skip_fft=False):
+def transfer_function_exact(n: int, dx: float, wl: float, dz: float) -> np.ndarray:
+    """The transfer function with the phase c * fx^2 evaluated without
+    intermediate rounding (long double, reduced mod 2 pi) for the reference's
+    c = fl(fl(pi wl) dz). Differs from ``transfer_function`` by the reference's
+    own rounding of fx and fx^2 (a few ulp of phases up to ~1e7 rad)."""
+    ks = signed_fft_index(n).astype(np.longdouble)
+    c = np.longdouble(float((np.pi * wl) * dz))
+    th = c * (ks / (np.longdouble(n) * np.longdouble(dx))) ** 2
+    two_pi = np.longdouble("6.283185307179586476925286766559005768")
+    th = (th - np.round(th / two_pi) * two_pi).astype(np.float64)
+    return np.exp(-1j * 2 * np.pi / wl * dz) * np.exp(1j * th)
+
+
+def propagate(u, U, sim: Sim, dz: float, cutoff_freq: float, skip_fft=False, exact_phase=False):
     """``propagate`` (big-wave/propagation.py:100-138). Returns (u_new, U_new)
     with ``U_new`` the spectrum of ``u_new`` as in the reference."""
     if not skip_fft:
         U = spfft.fft(u)
     # ``chunk *= H``: computed in complex128, stored in the field's dtype
-    U = (U * transfer_function(len(u), sim.dx, sim.wl, dz)).astype(U.dtype, copy=False)
+    tf = transfer_function_exact if exact_phase else transfer_function
+    U = (U * tf(len(u), sim.dx, sim.wl, dz)).astype(U.dtype, copy=False)
     rng = cutoff_zero_range(len(u), cutoff_freq, sim.dx)
     if rng is not None:
         U[rng[0]:rng[1]] = 0

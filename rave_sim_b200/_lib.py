@@ -118,6 +118,7 @@ SIGNATURES = {
     "rsw_sim_run": (C.c_int, [_P, C.POINTER(Source), C.POINTER(SourceRun), _P]),
     "rsw_sim_reset": (C.c_int, [_P, _P]),
     "rsw_sim_read": (C.c_int, [_P, _DP, _P]),
+    "rsw_sim_read_device": (C.c_int, [_P, _DP, _P]),
     "rsw_sim_accumulator": (C.c_int, [_P, C.POINTER(_DP)]),
     "rsw_sim_final_field": (C.c_int, [_P, _P, _P]),
     "rsw_sim_set_timing": (C.c_int, [_P, C.c_int]),

@@ -28,8 +28,8 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
 ]
 
-SOURCES = ["rsw_kernels.cu", "rsw_host.cpp"]
-HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h"]
+SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_kernels.cu", "rsw_host.cpp"]
+HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh"]
 
 
 def nvcc() -> str:
@@ -47,9 +47,11 @@ def _stale(target: Path, deps) -> bool:
 
 
 def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False) -> Path:
+    from concurrent.futures import ThreadPoolExecutor
+
     BUILD.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [INCLUDE / "rsw.h"]
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         s = CSRC / src
         o = BUILD / (s.stem + ".o")
@@ -58,13 +60,23 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
             cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(INCLUDE), "-I", str(CSRC), "-c", str(s), "-o", str(o)]
             if ptxas_verbose and s.suffix == ".cu":
                 cmd.insert(1, "-Xptxas=-v")
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0 or (verbose and r.stderr):
-                sys.stderr.write(r.stdout + r.stderr)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed on {src}")
+            jobs.append((src, cmd))
+
+    def run(job):
+        src, cmd = job
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, cmd, r
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(run, jobs))
+    for src, cmd, r in results:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        if r.returncode != 0 or (verbose and r.stderr):
+            sys.stderr.write(r.stdout + r.stderr)
+    for src, cmd, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}")
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart"]
         if verbose:

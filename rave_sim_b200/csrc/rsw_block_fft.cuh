@@ -13,6 +13,15 @@
 //     (beta >> ls) * R*S + (beta & (S-1)) + q*S,   q = 0..R-1
 // and is done by one thread, which reads and writes the same positions, so
 // stages exchange data through shared memory with one barrier each.
+//
+// Inside a butterfly the radix-R DFT is a radix-2 network in registers: the
+// forward network takes natural order and leaves bit-reversed order (register
+// brev(q) holds output q), the inverse network takes bit-reversed order and
+// leaves natural order, so no register permutation is ever needed.
+//
+// Twiddles W_{RS}^{jq} of stage s live in shared memory, loaded once per CTA:
+// a direct table [(q-1)*S + j] for strides S <= 256, otherwise two factors
+// W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64 entries per q.
 // Shared memory holds the C sequences with one pad element per 16 (phys(p))
 // and a per-sequence pitch chosen so that the accesses of one wavefront hit
 // distinct banks.
@@ -49,6 +58,7 @@ __host__ __device__ constexpr int brev_bits(int q, int bits) {
     for (int b = 0; b < bits; ++b) r |= ((q >> b) & 1) << (bits - 1 - b);
     return r;
 }
+__host__ __device__ constexpr int ilog2(int r) { return r <= 1 ? 0 : 1 + ilog2(r >> 1); }
 
 // x * W16^e with W16 = exp(DIR * 2 pi i / 16), e in [0, 8), e known after unrolling.
 template <int DIR, typename C> __device__ __forceinline__ C tw16(C x, int e) {
@@ -69,9 +79,8 @@ template <int DIR, typename C> __device__ __forceinline__ C tw16(C x, int e) {
     }
 }
 
-// In-register DFT of size R (2..16) on v[0..R-1], natural order in and out.
-// DIR = -1: forward (exp(-2 pi i jk/R)); DIR = +1: inverse, unnormalised.
-template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C *v) {
+// Radix-2 decimation-in-frequency network: natural order in, bit-reversed out.
+template <int R, int DIR, typename C> __device__ __forceinline__ void net_dif(C *v) {
 #pragma unroll
     for (int span = R / 2; span >= 1; span >>= 1) {
 #pragma unroll
@@ -84,32 +93,47 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void dft(C *v) 
             }
         }
     }
-    constexpr int bits = (R == 2) ? 1 : (R == 4) ? 2 : (R == 8) ? 3 : 4;
-    C t[R];
+}
+// Radix-2 decimation-in-time network: bit-reversed order in, natural out.
+template <int R, int DIR, typename C> __device__ __forceinline__ void net_dit(C *v) {
 #pragma unroll
-    for (int q = 0; q < R; ++q) t[q] = v[brev_bits(q, bits)];
+    for (int span = 1; span < R; span <<= 1) {
 #pragma unroll
-    for (int q = 0; q < R; ++q) v[q] = t[q];
+        for (int start = 0; start < R; start += 2 * span) {
+#pragma unroll
+            for (int k = 0; k < span; ++k) {
+                C a = v[start + k], b = tw16<DIR>(v[start + k + span], k * (8 / span));
+                v[start + k] = cadd(a, b);
+                v[start + k + span] = csub(a, b);
+            }
+        }
+    }
 }
 
-// Radix structure of a block of length 2^LOG_L.
-template <int LOG_L> struct Radix {
+// Radix structure of a block of length 2^LOG_L with E_ elements per thread
+// (the stage structure and twiddle layout do not depend on E_).
+template <int LOG_L, int E_ = 16> struct Radix {
     static_assert(LOG_L >= 4, "blocks hold at least 16 elements");
+    static_assert(E_ == 16 || E_ == 32, "16 or 32 elements per thread");
     static constexpr int L = 1 << LOG_L;
-    static constexpr int E = 16;
+    static constexpr int E = E_;
     static constexpr int T = L / E;  // threads per sequence
     static constexpr int NS = (LOG_L + 3) / 4;
     static constexpr int LR0 = LOG_L - 4 * (NS - 1);
     __host__ __device__ static constexpr int lr(int s) { return s == 0 ? LR0 : 4; }
     __host__ __device__ static constexpr int ls(int s) { return LOG_L - LR0 - 4 * s; }
-    // offset of stage s in the concatenated block twiddle table
-    // (entries [(q-1)*S + j] = W_{R*S}^{j*q}, q = 1..R-1, j < S)
-    __host__ __device__ static constexpr int64_t twoff(int s) {
-        int64_t o = 0;
-        for (int t = 0; t < s; ++t) o += int64_t((1 << lr(t)) - 1) << ls(t);
+    __host__ __device__ static constexpr bool direct(int s) { return ls(s) <= 8; }
+    __host__ __device__ static constexpr int tw_entries(int s) {
+        return s >= NS - 1 ? 0
+               : direct(s) ? ((1 << lr(s)) - 1) << ls(s)
+                           : ((1 << lr(s)) - 1) * (64 + (1 << (ls(s) - 6)));
+    }
+    __host__ __device__ static constexpr int twoff(int s) {
+        int o = 0;
+        for (int t = 0; t < s; ++t) o += tw_entries(t);
         return o;
     }
-    static constexpr int64_t twsize = twoff(NS - 1);  // last stage has no twiddles
+    static constexpr int TW = twoff(NS - 1) > 0 ? twoff(NS - 1) : 1;
 };
 
 // Digit reversal of a block position for a block of length 2^log_l (runtime
@@ -144,8 +168,8 @@ __host__ __device__ inline int64_t digitpos_rt(int64_t f, int log_l) {
     return p;
 }
 
-template <typename Real, int LOG_L, int C> struct Block : Radix<LOG_L> {
-    using Rx = Radix<LOG_L>;
+template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG_L, E_> {
+    using Rx = Radix<LOG_L, E_>;
     using Cx = typename CxT<Real>::T;
     using Rx::E;
     using Rx::L;
@@ -156,7 +180,9 @@ template <typename Real, int LOG_L, int C> struct Block : Radix<LOG_L> {
     static constexpr int BASE = L + L / 16;
     static constexpr int WANT = (C >= W) ? 1 : W / C;
     static constexpr int PITCH = BASE + (((WANT - BASE) % W) + W) % W;
-    static constexpr size_t SMEM = size_t(C) * PITCH * sizeof(Cx);
+    static constexpr size_t DATA = size_t(C) * PITCH * sizeof(Cx);
+    static constexpr size_t SMEM = DATA + size_t(Rx::TW) * sizeof(Cx);
+    static constexpr int RL = 1 << Rx::lr(NS - 1);  // radix of the last stage
 
     __device__ static __forceinline__ int phys(int p) { return p + (p >> 4); }
 
@@ -167,83 +193,117 @@ template <typename Real, int LOG_L, int C> struct Block : Radix<LOG_L> {
         const int b = beta >> LSS;
         return (b << (LRS + LSS)) + j + (q << LSS);
     }
+    // register holding position q of butterfly i: natural or bit-reversed layout
+    template <int s, bool BR> __device__ static constexpr int reg(int i, int q) {
+        constexpr int R = 1 << Rx::lr(s);
+        return i * R + (BR ? brev_bits(q, Rx::lr(s)) : q);
+    }
 
-    template <int s> __device__ static __forceinline__ void st(Cx *sm, int tp, const Cx *v) {
+    template <int s, bool BR> __device__ static __forceinline__ void st(Cx *sm, int tp, const Cx *v) {
         constexpr int R = 1 << Rx::lr(s);
 #pragma unroll
         for (int i = 0; i < E / R; ++i)
 #pragma unroll
-            for (int q = 0; q < R; ++q) sm[phys(pos<s>(tp, i, q))] = v[i * R + q];
+            for (int q = 0; q < R; ++q) sm[phys(pos<s>(tp, i, q))] = v[reg<s, BR>(i, q)];
     }
-    template <int s> __device__ static __forceinline__ void ld(const Cx *sm, int tp, Cx *v) {
+    template <int s, bool BR> __device__ static __forceinline__ void ld(const Cx *sm, int tp, Cx *v) {
         constexpr int R = 1 << Rx::lr(s);
 #pragma unroll
         for (int i = 0; i < E / R; ++i)
 #pragma unroll
-            for (int q = 0; q < R; ++q) v[i * R + q] = sm[phys(pos<s>(tp, i, q))];
+            for (int q = 0; q < R; ++q) v[reg<s, BR>(i, q)] = sm[phys(pos<s>(tp, i, q))];
     }
 
-    // forward stage s: DFT_R then twiddle W_{RS}^{j q}
-    template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Cx *__restrict__ tw) {
+    // twiddle W_{RS}^{j q} of stage s from the shared-memory tables
+    template <int s> __device__ static __forceinline__ Cx twid(const Cx *tw, int j, int q) {
+        constexpr int LSS = Rx::ls(s);
+        const Cx *t = tw + Rx::twoff(s);
+        if constexpr (Rx::direct(s)) {
+            return t[((q - 1) << LSS) + j];
+        } else {
+            constexpr int R = 1 << Rx::lr(s);
+            const Cx a = t[(q - 1) * 64 + (j & 63)];
+            const Cx b = t[(R - 1) * 64 + (q - 1) * (1 << (LSS - 6)) + (j >> 6)];
+            return cmul(a, b);
+        }
+    }
+
+    // forward stage s: natural in -> radix-R DFT -> bit-reversed out, twiddled
+    template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Cx *tw) {
         constexpr int R = 1 << Rx::lr(s);
         constexpr int LSS = Rx::ls(s);
 #pragma unroll
         for (int i = 0; i < E / R; ++i) {
-            dft<R, -1>(v + i * R);
+            net_dif<R, -1>(v + i * R);
             if constexpr (s < NS - 1) {
                 const int j = (tp + T * i) & ((1 << LSS) - 1);
-                const Cx *t = tw + Rx::twoff(s) + j;
 #pragma unroll
-                for (int q = 1; q < R; ++q) v[i * R + q] = cmul(v[i * R + q], __ldg(t + (int64_t(q - 1) << LSS)));
+                for (int q = 1; q < R; ++q) {
+                    Cx &x = v[reg<s, true>(i, q)];
+                    x = cmul(x, twid<s>(tw, j, q));
+                }
             }
         }
     }
-    // inverse stage s: conjugate twiddle then inverse DFT_R
-    template <int s> __device__ static __forceinline__ void dit(int tp, Cx *v, const Cx *__restrict__ tw) {
+    // inverse stage s: bit-reversed in -> conjugate twiddle -> inverse DFT -> natural out
+    template <int s> __device__ static __forceinline__ void dit(int tp, Cx *v, const Cx *tw) {
         constexpr int R = 1 << Rx::lr(s);
         constexpr int LSS = Rx::ls(s);
 #pragma unroll
         for (int i = 0; i < E / R; ++i) {
             if constexpr (s < NS - 1) {
                 const int j = (tp + T * i) & ((1 << LSS) - 1);
-                const Cx *t = tw + Rx::twoff(s) + j;
 #pragma unroll
-                for (int q = 1; q < R; ++q) v[i * R + q] = cmulc(v[i * R + q], __ldg(t + (int64_t(q - 1) << LSS)));
+                for (int q = 1; q < R; ++q) {
+                    Cx &x = v[reg<s, true>(i, q)];
+                    x = cmulc(x, twid<s>(tw, j, q));
+                }
             }
-            dft<R, +1>(v + i * R);
+            net_dit<R, +1>(v + i * R);
         }
     }
 
-    // Full forward transform starting from stage-0 positions in registers;
-    // ends with the values at last-stage positions in registers.
+    // Full forward transform from stage-0 positions (natural layout) to
+    // last-stage positions (bit-reversed layout) in registers.
     template <int s = 0> __device__ static __forceinline__ void forward(Cx *sm, int tp, Cx *v, const Cx *tw) {
         dif<s>(tp, v, tw);
         if constexpr (s < NS - 1) {
-            st<s>(sm, tp, v);
+            st<s, true>(sm, tp, v);
             __syncthreads();
-            ld<s + 1>(sm, tp, v);
+            ld<s + 1, false>(sm, tp, v);
             forward<s + 1>(sm, tp, v, tw);
         }
     }
-    // Full inverse transform from last-stage positions to stage-0 positions.
+    // Full inverse transform from last-stage positions (bit-reversed layout)
+    // to stage-0 positions (natural layout).
     template <int s = NS - 1> __device__ static __forceinline__ void inverse(Cx *sm, int tp, Cx *v, const Cx *tw) {
         dit<s>(tp, v, tw);
         if constexpr (s > 0) {
-            st<s>(sm, tp, v);
+            st<s, false>(sm, tp, v);
             __syncthreads();
-            ld<s - 1>(sm, tp, v);
+            ld<s - 1, true>(sm, tp, v);
             inverse<s - 1>(sm, tp, v, tw);
         }
     }
 
-    // Position held by register (i, q) at the first / last stage.
+    // position held by register r in the natural layout of stage 0 and in the
+    // bit-reversed layout of the last stage
     __device__ static __forceinline__ int first_pos(int tp, int r) {
         constexpr int R = 1 << Rx::lr(0);
         return pos<0>(tp, r / R, r % R);
     }
     __device__ static __forceinline__ int last_pos(int tp, int r) {
-        constexpr int R = 1 << Rx::lr(NS - 1);
-        return pos<NS - 1>(tp, r / R, r % R);
+        constexpr int LRL = Rx::lr(NS - 1);
+        return pos<NS - 1>(tp, r / RL, brev_bits(r % RL, LRL));
+    }
+    // digit-reversed frequency index of last_pos(tp, r)
+    __device__ static __forceinline__ int last_freq(int tp, int r) {
+        return int(digitrev_rt(last_pos(tp, r), LOG_L));
+    }
+
+    // copy the block's twiddle tables (global, host-built layout) into shared memory
+    __device__ static __forceinline__ void load_twiddles(Cx *tw_sm, const Cx *__restrict__ tw_g) {
+        for (int k = threadIdx.x; k < Rx::TW; k += NT) tw_sm[k] = tw_g[k];
     }
 };
 

@@ -1,0 +1,52 @@
+// Column-pass kernels and row chirp tables (both precisions).
+#include "rsw_passes.cuh"
+
+namespace rsw {
+#define RSW_COL_CASE(R, L, C) \
+    case L: return e == 32 ? col_impl<R, L, C, 32>(a, s) : col_impl<R, L, C, 16>(a, s);
+#define RSW_COL_CASE16(R, L, C) \
+    case L: return col_impl<R, L, C, 16>(a, s);
+
+
+cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) {
+    if (dbl) {
+        switch (a.log_n1) {
+            RSW_COL_CASE16(double, 4, 4) RSW_COL_CASE16(double, 5, 4) RSW_COL_CASE16(double, 6, 4)
+            RSW_COL_CASE16(double, 7, 4) RSW_COL_CASE16(double, 8, 4) RSW_COL_CASE(double, 9, 4)
+            RSW_COL_CASE(double, 10, 4) RSW_COL_CASE(double, 11, 4)
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (a.log_n1) {
+        RSW_COL_CASE16(float, 4, 4) RSW_COL_CASE16(float, 5, 4) RSW_COL_CASE16(float, 6, 4)
+        RSW_COL_CASE16(float, 7, 4) RSW_COL_CASE16(float, 8, 4) RSW_COL_CASE(float, 9, 4)
+        RSW_COL_CASE(float, 10, 4) RSW_COL_CASE(float, 11, 4) RSW_COL_CASE(float, 12, 4)
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+
+#define RSW_CH_CASE(R, L) \
+    case L: return e == 32 ? chirp_impl<R, L, 32>(out, hi, lo, s) : chirp_impl<R, L, 16>(out, hi, lo, s);
+#define RSW_CH_CASE16(R, L) \
+    case L: return chirp_impl<R, L, 16>(out, hi, lo, s);
+
+cudaError_t launch_chirp_table(void *out, int log_n2, double hi, double lo, bool dbl, int e, cudaStream_t s) {
+    if (dbl) {
+        switch (log_n2) {
+            RSW_CH_CASE16(double, 4) RSW_CH_CASE16(double, 5) RSW_CH_CASE16(double, 6) RSW_CH_CASE16(double, 7)
+            RSW_CH_CASE16(double, 8) RSW_CH_CASE(double, 9) RSW_CH_CASE(double, 10) RSW_CH_CASE(double, 11)
+            RSW_CH_CASE(double, 12) RSW_CH_CASE(double, 13)
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (log_n2) {
+        RSW_CH_CASE16(float, 4) RSW_CH_CASE16(float, 5) RSW_CH_CASE16(float, 6) RSW_CH_CASE16(float, 7)
+        RSW_CH_CASE16(float, 8) RSW_CH_CASE(float, 9) RSW_CH_CASE(float, 10) RSW_CH_CASE(float, 11)
+        RSW_CH_CASE(float, 12) RSW_CH_CASE(float, 13) RSW_CH_CASE(float, 14)
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+
+}  // namespace rsw

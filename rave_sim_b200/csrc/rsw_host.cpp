@@ -15,6 +15,7 @@
 #include <complex>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -24,8 +25,8 @@
 #include "rsw_internal.h"
 
 namespace rsw {
-cudaError_t launch_row_pass(const PassArgs &a, bool dbl, cudaStream_t s);
-cudaError_t launch_col_pass(const PassArgs &a, bool dbl, cudaStream_t s);
+cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
+cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
                                    cudaStream_t s);
 cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
@@ -39,6 +40,7 @@ cudaError_t launch_detect(const void *u, const int64_t *bounds, const double *co
                           double weight, bool dbl, cudaStream_t s);
 cudaError_t launch_zero(double *p, int64_t n, cudaStream_t s);
 cudaError_t launch_fill_ones(void *u, int64_t n, bool dbl, cudaStream_t s);
+cudaError_t launch_chirp_table(void *out, int log_n2, double hi, double lo, bool dbl, int e, cudaStream_t s);
 unsigned long long launch_count();
 }  // namespace rsw
 
@@ -119,6 +121,7 @@ static PropArgs make_prop(int64_t n, double dx, double wl, double dz, double cut
     p.A = make_double2(std::cos(phi), std::sin(phi));
     p.fac = 1.0 / double(n);
     p.dx = dx;
+    p.rdx = 1.0 / dx;
     const double frac = cutoff_freq * dx;
     const double start = std::ceil(double(n) * frac);
     if (!(start > double(n) / 2.0)) {
@@ -127,6 +130,19 @@ static PropArgs make_prop(int64_t n, double dx, double wl, double dz, double cut
         p.cut_hi = std::min<int64_t>(n - int64_t(start) + 1, n);
     }
     return p;
+}
+
+// Chirp form of the transfer-function phase for two-level plans: theta =
+// c fx^2 with fx = ks / (N dx) exactly, i.e. G ks^2 turns with
+// G = c / (2 pi N^2 dx^2), evaluated in long double and split into a
+// double-double (c is the reference's rounded fl(fl(pi wl) dz)).
+static void chirp_constant(const PropArgs &p, int64_t n, double *g_hi, double *g_lo) {
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    const long double ldx = (long double)p.dx;
+    const long double nn = (long double)n;
+    const long double g = (long double)p.c / (two_pi * nn * nn * ldx * ldx);
+    *g_hi = double(g);
+    *g_lo = double(g - (long double)(*g_hi));
 }
 
 // np.linspace chunk coordinates of generate_grating_chunk
@@ -270,7 +286,8 @@ struct rsw_plan_s {
     int dtype = RSW_C128;
     int log_n1 = 0, log_n2 = 0;  // column level, row level
     int device = 0;
-    DevBuf tw_row, tw_col, tw4_lo, tw4_hi, tw4_hi_inv;
+    int row_e = 16, col_e = 16;  // elements per thread of the row / column kernels
+    DevBuf tw_row, tw_col, tw4_lo, tw4_hi;
     int tw4_shift = 0;
     DevBuf scratch;                                       // N samples, for the natural-order APIs
     DevBuf det_bounds, det_cos, det_r;                    // cached detector geometry
@@ -278,6 +295,7 @@ struct rsw_plan_s {
     int64_t det_npix = -1;
     DevBuf chunk_xs, chunk_st;                            // per-call chunk tables
     DevBuf sample_grid, sample_db, sample_fac;            // per-call sample row data
+    DevBuf h3_call;                                       // per-call chirp table
     bool dbl() const { return dtype == RSW_C128; }
     size_t elem() const { return dbl() ? 16 : 8; }
 };
@@ -295,18 +313,29 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
     v.push_back(T(c.imag()));
 }
 
-// Block twiddle table of a block of length 2^log_l (layout of Radix<LOG_L>::twoff).
+// Block twiddle tables of a block of length 2^log_l, in the shared-memory
+// layout of Radix<LOG_L>: per stage s (all but the last), W_{RS}^{jq} for
+// q = 1..R-1, j < S, either direct [(q-1)*S + j] (S <= 256) or factored as
+// W^{(j & 63) q} [(q-1)*64 + (j & 63)] and W^{64 (j >> 6) q} [(R-1)*64 + (q-1)*(S/64) + (j >> 6)].
 template <typename T> static std::vector<T> block_twiddles(int log_l) {
     std::vector<T> v;
-    if (log_l < 4) return v;
-    const int ns = (log_l + 3) / 4;
-    const int lr0 = log_l - 4 * (ns - 1);
-    for (int s = 0; s < ns - 1; ++s) {
-        const int lr = s == 0 ? lr0 : 4;
-        const int ls = log_l - lr0 - 4 * s;
-        const int64_t R = int64_t(1) << lr, S = int64_t(1) << ls;
-        for (int64_t q = 1; q < R; ++q)
-            for (int64_t j = 0; j < S; ++j) push_c(v, twiddle(j * q, R * S));
+    if (log_l >= 4) {
+        const int ns = (log_l + 3) / 4;
+        const int lr0 = log_l - 4 * (ns - 1);
+        for (int s = 0; s < ns - 1; ++s) {
+            const int lr = s == 0 ? lr0 : 4;
+            const int ls = log_l - lr0 - 4 * s;
+            const int64_t R = int64_t(1) << lr, S = int64_t(1) << ls;
+            if (ls <= 8) {
+                for (int64_t q = 1; q < R; ++q)
+                    for (int64_t j = 0; j < S; ++j) push_c(v, twiddle(j * q, R * S));
+            } else {
+                for (int64_t q = 1; q < R; ++q)
+                    for (int64_t j = 0; j < 64; ++j) push_c(v, twiddle(j * q, R * S));
+                for (int64_t q = 1; q < R; ++q)
+                    for (int64_t j = 0; j < S / 64; ++j) push_c(v, twiddle(64 * j * q, R * S));
+            }
+        }
     }
     if (v.empty()) push_c(v, cplx(1, 0));
     return v;
@@ -316,19 +345,14 @@ template <typename T> static rsw_status plan_tables(rsw_plan_s *p) {
     CHECK(p->tw_row.upload(block_twiddles<T>(p->log_n2)));
     if (p->log_n1 > 0) {
         CHECK(p->tw_col.upload(block_twiddles<T>(p->log_n1)));
+        // four-step twiddles in FP64 for both dtypes (rounded per tile on the device)
         const int h = (p->log_n + 1) / 2;
         p->tw4_shift = h;
-        std::vector<T> lo, hi, hinv;
+        std::vector<double> lo, hi;
         for (int64_t a = 0; a < (int64_t(1) << h); ++a) push_c(lo, twiddle(a, p->n));
-        const double inv_n = 1.0 / double(p->n);
-        for (int64_t b = 0; b < (int64_t(1) << (p->log_n - h)); ++b) {
-            const cplx w = twiddle(b << h, p->n);
-            push_c(hi, w);
-            push_c(hinv, std::conj(w) * inv_n);
-        }
+        for (int64_t b = 0; b < (int64_t(1) << (p->log_n - h)); ++b) push_c(hi, twiddle(b << h, p->n));
         CHECK(p->tw4_lo.upload(lo));
         CHECK(p->tw4_hi.upload(hi));
-        CHECK(p->tw4_hi_inv.upload(hinv));
     }
     return RSW_OK;
 }
@@ -346,6 +370,10 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *l2)
     } else {
         int a = std::min(col_max, lg / 2);
         int b = lg - a;
+        if (b < 7) {  // rows of two-level plans hold at least 2^7 samples
+            b = 7;
+            a = lg - b;
+        }
         if (b > row_max) {
             a = lg - row_max;
             b = row_max;
@@ -353,11 +381,36 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *l2)
         if (a > col_max || a < 4)
             return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the two-level limit 2^%d for this dtype", lg,
                         row_max + col_max);
+        // RSW_SPLIT overrides the column level (tuning sweeps) when valid
+        const char *ov = std::getenv("RSW_SPLIT");
+        if (ov && *ov) {
+            const int oa = std::atoi(ov), ob = lg - oa;
+            if (oa >= 4 && oa <= col_max && ob >= 7 && ob <= row_max) {
+                a = oa;
+                b = ob;
+            }
+        }
         *l1 = a;
         *l2 = b;
     }
     *log_n = lg;
     return RSW_OK;
+}
+
+// Kernel variant per block size: elements per thread (16 or 32). 32 halves the
+// threads of a CTA and lifts the register cap of the large blocks.
+// RSW_ROW_E / RSW_COL_E override the choice (tuning sweeps).
+static int env_int(const char *name, int dflt) {
+    const char *v = std::getenv(name);
+    return v && *v ? std::atoi(v) : dflt;
+}
+static void choose_tuning(rsw_plan_s *p) {
+    auto pick = [](int log_l, int dflt) { return log_l >= 9 ? dflt : 16; };
+    p->row_e = pick(p->log_n2, 16);
+    p->col_e = pick(p->log_n1, 16);
+    const int re = env_int("RSW_ROW_E", 0), ce = env_int("RSW_COL_E", 0);
+    if ((re == 16 || re == 32) && p->log_n2 >= 9) p->row_e = re;
+    if ((ce == 16 || ce == 32) && p->log_n1 >= 9) p->col_e = ce;
 }
 
 static PassArgs base_args(const rsw_plan_s *p) {
@@ -369,7 +422,6 @@ static PassArgs base_args(const rsw_plan_s *p) {
     a.tw_col = p->tw_col.p;
     a.tw4_lo = p->tw4_lo.p;
     a.tw4_hi = p->tw4_hi.p;
-    a.tw4_hi_inv = p->tw4_hi_inv.p;
     a.tw4_shift = p->tw4_shift;
     a.pr.fac = 1.0 / double(p->n);
     a.tr.kind = TR_NONE;
@@ -431,7 +483,7 @@ struct TimingLog {
 static rsw_status run_row(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s, TimingLog *tl = nullptr) {
     TimingLog::Rec r{};
     if (tl && tl->enabled) tl->begin(0, s, r);
-    cudaError_t e = launch_row_pass(a, p->dbl(), s);
+    cudaError_t e = launch_row_pass(a, p->dbl(), p->row_e, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "row pass (2^%d): %s", a.log_n2, cudaGetErrorString(e));
     if (tl && tl->enabled) tl->end(r, s);
     return RSW_OK;
@@ -439,9 +491,25 @@ static rsw_status run_row(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s
 static rsw_status run_col(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s, TimingLog *tl = nullptr) {
     TimingLog::Rec r{};
     if (tl && tl->enabled) tl->begin(1, s, r);
-    cudaError_t e = launch_col_pass(a, p->dbl(), s);
+    cudaError_t e = launch_col_pass(a, p->dbl(), p->col_e, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "column pass (2^%d): %s", a.log_n1, cudaGetErrorString(e));
     if (tl && tl->enabled) tl->end(r, s);
+    return RSW_OK;
+}
+
+// Build the row-level chirp table of a transfer function into `table` (N2
+// samples) and switch `pr` to the chirp form. Two-level plans only.
+static rsw_status prepare_chirp(const rsw_plan_s *p, PropArgs &pr, void *table, cudaStream_t s) {
+    if (p->log_n1 == 0 || !pr.has_h) return RSW_OK;
+    double g_hi, g_lo;
+    chirp_constant(pr, p->n, &g_hi, &g_lo);
+    const double n1sq = std::ldexp(1.0, 2 * p->log_n1);  // exact power of two
+    cudaError_t e = launch_chirp_table(table, p->log_n2, g_hi * n1sq, g_lo * n1sq, p->dbl(), p->row_e, s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "chirp table: %s", cudaGetErrorString(e));
+    pr.chirp = 1;
+    pr.g_hi = g_hi;
+    pr.g_lo = g_lo;
+    pr.h3 = table;
     return RSW_OK;
 }
 
@@ -476,6 +544,7 @@ rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
     p->log_n1 = l1;
     p->log_n2 = l2;
     CU(cudaGetDevice(&p->device));
+    choose_tuning(p.get());
     CHECK(p->dbl() ? plan_tables<double>(p.get()) : plan_tables<float>(p.get()));
     *out = p.release();
     return RSW_OK;
@@ -554,6 +623,10 @@ rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, dou
     PassArgs a = base_args(p);
     a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0);
     const bool two = p->log_n1 > 0;
+    if (two && a.pr.has_h) {
+        CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_n2) * p->elem()));
+        CHECK(prepare_chirp(p, a.pr, p->h3_call.p, s));
+    }
     // 1. spectrum of u in the internal layout, in place in u
     if (skip_fft) {
         cudaError_t e = launch_natural_to_spec(U, u, p->n, p->log_n1, p->log_n2, p->dbl(), s);
@@ -618,6 +691,7 @@ rsw_status rsw_apply_grating_factors(rsw_plan p, void *u, double dx, int64_t chu
     TransArgs tr{};
     tr.kind = TR_GRATING;
     tr.pitch0 = pitch;
+    tr.inv_pitch0 = 1.0 / pitch;
     tr.dc0 = dc;
     tr.half_dc0 = dc / 2;
     tr.fa = make_double2(fa[0], fa[1]);
@@ -637,6 +711,8 @@ rsw_status rsw_apply_dba_grating_factors(rsw_plan p, void *u, double dx, int64_t
     tr.kind = TR_DBA;
     tr.pitch0 = pitch0;
     tr.pitch1 = pitch1;
+    tr.inv_pitch0 = 1.0 / pitch0;
+    tr.inv_pitch1 = 1.0 / pitch1;
     tr.dc0 = dc0;
     tr.half_dc0 = dc0 / 2;
     tr.dc1 = dc1;
@@ -798,6 +874,7 @@ struct rsw_sim_s {
     DevBuf acc, comp;
     DevBuf buf[2];
     DevBuf mat_db, mat_fac;  // per-run sample material tables
+    std::vector<std::unique_ptr<DevBuf>> h3_pool;  // chirp tables, one per distinct dz of a run
     int last_field = -1;
     TimingLog tl;
     int64_t split_steps = 0;
@@ -819,6 +896,29 @@ struct Runner {
     int readonly = -1;      // buffer that must not be written (snapshot)
     // per-run material factors: per element [fa? ...]
     std::vector<std::vector<cplx>> db;  // deltabeta per element (gratings: a,b,sub; samples: materials 1..)
+    std::vector<double> chirp_dz;       // dz of each built chirp table of this run (slot = index)
+
+    // chirp table for a distance dz at this run's wavelength (built on first use)
+    rsw_status chirp_for(PropArgs &pr, double dz) {
+        if (P->log_n1 == 0 || !pr.has_h) return RSW_OK;
+        size_t slot = 0;
+        while (slot < chirp_dz.size() && chirp_dz[slot] != dz) ++slot;
+        const bool fresh = slot == chirp_dz.size();
+        if (fresh) {
+            chirp_dz.push_back(dz);
+            if (S->h3_pool.size() <= slot) S->h3_pool.emplace_back(new DevBuf());
+            CHECK(S->h3_pool[slot]->alloc(size_t(int64_t(1) << P->log_n2) * P->elem()));
+            CHECK(prepare_chirp(P, pr, S->h3_pool[slot]->p, st));
+            return RSW_OK;
+        }
+        double g_hi, g_lo;
+        chirp_constant(pr, P->n, &g_hi, &g_lo);
+        pr.chirp = 1;
+        pr.g_hi = g_hi;
+        pr.g_lo = g_lo;
+        pr.h3 = S->h3_pool[slot]->p;
+        return RSW_OK;
+    }
 
     int target() const {
         if (cur < 0) return readonly == 0 ? 1 : 0;
@@ -830,6 +930,7 @@ struct Runner {
         PassArgs a = base_args(P);
         a.tr = tr;
         a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0);
+        CHECK(chirp_for(a.pr, dz));
         if (P->log_n1 > 0) {
             a.in = ones ? nullptr : S->buf[cur].p;
             a.out = S->buf[dst].p;
@@ -907,6 +1008,8 @@ struct Runner {
                 tr.fb = make_double2(fb.real(), fb.imag());
                 tr.pitch0 = e.pitch;
                 tr.pitch1 = e.pitch1;
+                tr.inv_pitch0 = 1.0 / e.pitch;
+                tr.inv_pitch1 = e.pitch1 > 0 ? 1.0 / e.pitch1 : 0.0;
                 tr.dc0 = (1.0 - zf) * e.dc[0] + zf * e.dc[1];
                 tr.half_dc0 = tr.dc0 / 2;
                 tr.dc1 = (1.0 - zf) * e.dc1[0] + zf * e.dc1[1];
@@ -1072,6 +1175,13 @@ rsw_status rsw_sim_read(rsw_sim S, double *h, void *stream) {
     const size_t n = size_t(S->nr_phase_steps * S->geom.n_pix);
     CU(cudaMemcpyAsync(h, S->acc.p, n * sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CU(cudaStreamSynchronize((cudaStream_t)stream));
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_read_device(rsw_sim S, double *d, void *stream) {
+    if (!S || !d) return fail(RSW_ERR_INVALID, "NULL argument");
+    const size_t n = size_t(S->nr_phase_steps * S->geom.n_pix);
+    CU(cudaMemcpyAsync(d, S->acc.p, n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return RSW_OK;
 }
 

@@ -21,6 +21,7 @@ struct TransArgs {
     double2 fa, fb;  // material factors
     // grating coordinates: per-chunk np.linspace (start, step)
     double pitch0, pitch1, half_dc0, dc0, dc1;
+    double inv_pitch0, inv_pitch1;       // 1/pitch (correctly rounded), for the corrected quotient
     int64_t chunk_size;  // >= N: single chunk
     double xstart0, step0;               // single-chunk values
     const double *chunk_xstart;          // per-chunk tables (device) when several chunks
@@ -46,7 +47,14 @@ struct PropArgs {
     double2 A;          // exp(-i 2 pi dz / wl)
     double fac;         // 1.0 / N
     double dx;
+    double rdx;         // 1.0 / dx
     int64_t cut_lo, cut_hi;  // zero natural frequency indices k in [cut_lo, cut_hi)
+    // Chirp form of the transfer function (two-level plans): phase in turns
+    // G * ks^2, G = c / (2 pi N^2 dx^2) as a double-double, ks = k1 + N1 k2s;
+    // h3 = exp(2 pi i G N1^2 k2s^2) in the row kernel's register order.
+    int chirp;
+    double g_hi, g_lo;
+    const void *h3;
 };
 
 enum PassFlags : int {
@@ -68,9 +76,8 @@ struct PassArgs {
     int flags;
     const void *tw_row;   // block twiddles of the row level
     const void *tw_col;   // block twiddles of the column level
-    const void *tw4_lo;   // four-step twiddles: W_N^m = lo[m & mask] * hi[m >> shift]
+    const void *tw4_lo;   // four-step twiddles (FP64): W_N^m = lo[m & mask] * hi[m >> shift]
     const void *tw4_hi;
-    const void *tw4_hi_inv;  // conj(hi) / N
     int tw4_shift;
     TransArgs tr;
     PropArgs pr;

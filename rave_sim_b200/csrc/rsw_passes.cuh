@@ -1,0 +1,490 @@
+// Split-step wavefront propagation kernels for B200 (sm_100a): device code
+// shared by the translation units rsw_row_f64.cu, rsw_row_f32.cu, rsw_col.cu
+// and rsw_kernels.cu.
+//
+// The field of N = N1 * N2 samples is viewed as N1 rows of N2 contiguous
+// samples. One split step (reference: big-wave/propagation.py:100-138 preceded
+// by a transmission multiply, big-wave/optical_element.py:134-206/:432-476)
+// is two passes over HBM:
+//
+//   column pass  one CTA per C adjacent columns: inverse column FFT of the
+//                previous step, transmission multiply at x(n), forward column
+//                FFT, four-step twiddle W_N^(n2*k1);
+//   row pass     one CTA per row: forward row FFT, Fresnel transfer function
+//                and frequency cutoff on the digit-reversed spectrum,
+//                inverse row FFT, conjugate twiddle and 1/N.
+//
+// Between steps the buffer holds the "mid" representation (after the row
+// pass); the field itself (natural order) only exists inside the column pass,
+// where the transmission needs it. Small fields (N <= one block) use a single
+// row pass per step.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rsw_block_fft.cuh"
+#include "rsw_internal.h"
+
+namespace rsw {
+
+// ---------------------------------------------------------------- counters
+__device__ __forceinline__ double rint_d(double x) { return rint(x); }
+
+// Range reduction of a phase to [-pi, pi] (Cody & Waite 1980, three-part
+// constant; 2pi = P1 + P2 + P3 with P1, P2 of 29 significant bits so that
+// k*P1 and k*P2 are exact for |k| < 2^24), then sincos of the remainder.
+__device__ __forceinline__ void sincos_phase(double th, double *s, double *c) {
+    const double P1 = 0x1.921fb54000000p+2;
+    const double P2 = 0x1.10b4612000000p-28;
+    const double P3 = -0x1.676733ae8fe48p-58;
+    const double INV2PI = 0x1.45f306dc9c883p-3;
+    const double k = rint_d(th * INV2PI);
+    if (fabs(k) < 16777216.0) {
+        double r = fma(-k, P1, th);
+        r = fma(-k, P2, r);
+        r = fma(-k, P3, r);
+        sincos(r, s, c);
+    } else {
+        sincos(th, s, c);
+    }
+}
+__device__ __forceinline__ double reduce_phase(double th) {
+    const double P1 = 0x1.921fb54000000p+2;
+    const double P2 = 0x1.10b4612000000p-28;
+    const double P3 = -0x1.676733ae8fe48p-58;
+    const double INV2PI = 0x1.45f306dc9c883p-3;
+    const double k = rint_d(th * INV2PI);
+    double r = fma(-k, P1, th);
+    r = fma(-k, P2, r);
+    return fma(-k, P3, r);
+}
+
+// ------------------------------------------------------------- transmission
+__device__ __forceinline__ double grating_x(const TransArgs &t, int64_t n) {
+    // np.linspace(x_start, x_stop, cnt, endpoint=False) of the chunk holding n:
+    // x = fl(fl(l * step) + x_start)   (big-wave/optical_element.py:352-354)
+    if (t.chunk_size <= 0) return __dadd_rn(__dmul_rn(double(n), t.step0), t.xstart0);
+    const int64_t ch = n / t.chunk_size;
+    const int64_t l = n - ch * t.chunk_size;
+    return __dadd_rn(__dmul_rn(double(l), __ldg(t.chunk_step + ch)), __ldg(t.chunk_xstart + ch));
+}
+
+// Correctly rounded x / d from the correctly rounded reciprocal r = 1/d and
+// one FMA correction (Markstein's theorem).
+__device__ __forceinline__ double div_rn(double x, double d, double r) {
+    const double q0 = x * r;
+    return fma(fma(-q0, d, x), r, q0);
+}
+
+// np.mod(x / p + off, 1) < dc  (np.mod(a, 1) == a - floor(a) for finite a)
+__device__ __forceinline__ bool mod_less(double x, double p, double rp, double off, double dc) {
+    const double a = __dadd_rn(div_rn(x, p, rp), off);
+    return __dsub_rn(a, floor(a)) < dc;
+}
+
+__device__ __forceinline__ double sample_row_x(const TransArgs &t, int64_t j) {
+    // row_x = np.arange(rowlen) * psx + x_pos - rowlen * psx * 0.5
+    return __dsub_rn(__dadd_rn(__dmul_rn(double(j), t.psx), t.sample_xpos), t.sample_hw);
+}
+
+static __device__ __noinline__ double2 sample_interp(const TransArgs &t, int64_t j, int m0, int m1, double x,
+                                              double xj);
+
+// Sample row factor at sample n: exp(i y * np.interp(x, row_x, row_db, 0, 0))
+// (big-wave/optical_element.py:452-472). Returns false for vacuum (factor 1).
+__device__ __forceinline__ bool sample_factor(const TransArgs &t, int64_t n, double2 *f) {
+    const double x = __dmul_rn(double(n) - t.half_n, t.dx);
+    const int64_t last = t.x_len - 1;
+    const double x0 = sample_row_x(t, 0);
+    const double xl = sample_row_x(t, last);
+    if (x < x0 || x > xl) return false;
+    int mi;
+    if (x == xl) {
+        mi = t.row_grid[last];
+        if (mi == 0) return false;
+        *f = t.mat_factor[mi];
+        return true;
+    }
+    int64_t j = int64_t(floor((x - x0) * t.sample_inv_psx));
+    j = j < 0 ? 0 : (j > last - 1 ? last - 1 : j);
+    // move to the bracket row_x[j] <= x < row_x[j+1] (bounded)
+    for (int it = 0; it < 4 && j > 0 && x < sample_row_x(t, j); ++it) --j;
+    for (int it = 0; it < 4 && j < last - 1 && x >= sample_row_x(t, j + 1); ++it) ++j;
+    const int m0 = t.row_grid[j];
+    const int m1 = t.row_grid[j + 1];
+    const double xj = sample_row_x(t, j);
+    if (m0 == m1 || x == xj) {
+        if (m0 == 0) return false;
+        *f = t.mat_factor[m0];
+        return true;
+    }
+    *f = sample_interp(t, j, m0, m1, x, xj);
+    return true;
+}
+
+// Interpolated delta+i*beta between two different pixels and its factor
+// exp(i y db); kept out of line (only samples at material boundaries get here).
+static __device__ __noinline__ double2 sample_interp(const TransArgs &t, int64_t j, int m0, int m1, double x,
+                                              double xj) {
+    const double2 d0 = t.mat_db[m0], d1 = t.mat_db[m1];
+    const double dxp = __dsub_rn(sample_row_x(t, j + 1), xj);
+    const double sre = __ddiv_rn(__dsub_rn(d1.x, d0.x), dxp);
+    const double sim = __ddiv_rn(__dsub_rn(d1.y, d0.y), dxp);
+    const double xr = __dsub_rn(x, xj);
+    const double dre = __dadd_rn(__dmul_rn(sre, xr), d0.x);
+    const double dim = __dadd_rn(__dmul_rn(sim, xr), d0.y);
+    // exp((0, y) * (dre, dim)) = exp(-y*dim) * (cos(y*dre), sin(y*dre))
+    const double amp = exp(-__dmul_rn(t.sample_y, dim));
+    double s, c;
+    sincos(__dmul_rn(t.sample_y, dre), &s, &c);
+    return make_double2(amp * c, amp * s);
+}
+
+__device__ __forceinline__ double2 to_c(double2 a, double2) { return a; }
+__device__ __forceinline__ float2 to_c(double2 a, float2) { return make_float2(float(a.x), float(a.y)); }
+
+template <typename Cx> __device__ __forceinline__ Cx apply_trans(const TransArgs &t, int64_t n, Cx u) {
+    switch (t.kind) {
+    case TR_SCALAR: return cmul(u, to_c(t.fa, u));
+    case TR_GRATING: {
+        const double x = grating_x(t, n);
+        const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0);
+        return cmul(u, to_c(m ? t.fa : t.fb, u));
+    }
+    case TR_DBA: {
+        const double x = grating_x(t, n);
+        const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0) &&
+                       mod_less(x, t.pitch1, t.inv_pitch1, 0.0, t.dc1);
+        return cmul(u, to_c(m ? t.fa : t.fb, u));
+    }
+    case TR_SAMPLE: {
+        double2 f;
+        if (!sample_factor(t, n, &f)) return u;
+        // computed in FP64, stored in the field's precision
+        const double2 ud = make_double2(double(u.x), double(u.y));
+        return to_c(cmul(ud, f), u);
+    }
+    default: return u;
+    }
+}
+
+// ------------------------------------------------------------ propagator
+// U *= exp(-i2pi dz/wl) * exp(i pi wl dz fx^2), fx = (ks * (1/N)) / dx, zero in
+// the cutoff range (big-wave/propagation.py:74-97, :124-137).
+// (ks * 2^-n) / dx == 2^-n * (ks / dx) exactly; ks / dx is the correctly
+// rounded quotient from the reciprocal and one FMA correction (Markstein).
+__device__ __forceinline__ double prop_phase(const PropArgs &p, int64_t ks) {
+    const double fx = __dmul_rn(div_rn(double(ks), p.dx, p.rdx), p.fac);
+    return __dmul_rn(p.c, __dmul_rn(fx, fx));
+}
+
+// frac((hi + lo) * m) in [-0.5, 0.5] for an integer-valued m < 2^53, with the
+// product error recovered by FMA (double-double argument, in turns).
+__device__ __forceinline__ double frac_dd(double hi, double lo, double m) {
+    const double p = hi * m;
+    const double e = fma(hi, m, -p);
+    double r = (p - rint(p)) + fma(lo, m, e);
+    return r - rint(r);
+}
+
+// exp(2 pi i t) for t in turns
+__device__ __forceinline__ double2 cis_turns(double t) {
+    double s, c;
+    sincospi(2.0 * t, &s, &c);
+    return make_double2(c, s);
+}
+__device__ __forceinline__ double2 prop_apply(const PropArgs &p, int64_t k, int64_t ks, double2 U) {
+    if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) return make_double2(0.0, 0.0);
+    if (!p.has_h) return U;
+    double s, c;
+    sincos_phase(prop_phase(p, ks), &s, &c);
+    const double2 H = make_double2(p.A.x * c - p.A.y * s, p.A.x * s + p.A.y * c);
+    return cmul(U, H);
+}
+__device__ __forceinline__ float2 prop_apply(const PropArgs &p, int64_t k, int64_t ks, float2 U) {
+    if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) return make_float2(0.f, 0.f);
+    if (!p.has_h) return U;
+    float s, c;
+    sincosf(float(reduce_phase(prop_phase(p, ks))), &s, &c);
+    const float ax = float(p.A.x), ay = float(p.A.y);
+    const float2 H = make_float2(ax * c - ay * s, ax * s + ay * c);
+    return cmul(U, H);
+}
+
+template <typename Cx> __device__ __forceinline__ Cx one_c();
+template <> __device__ __forceinline__ double2 one_c<double2>() { return make_double2(1.0, 0.0); }
+template <> __device__ __forceinline__ float2 one_c<float2>() { return make_float2(1.f, 0.f); }
+
+__device__ __forceinline__ double2 cvt(double2 a, double2) { return a; }
+__device__ __forceinline__ float2 cvt(double2 a, float2) { return make_float2(float(a.x), float(a.y)); }
+
+// W_N^m from the FP64 four-step tables (lo[m & mask] * hi[m >> shift]).
+__device__ __forceinline__ double2 w4(const PassArgs &a, int64_t m) {
+    const double2 *lo = static_cast<const double2 *>(a.tw4_lo);
+    const double2 *hi = static_cast<const double2 *>(a.tw4_hi);
+    const int64_t mask = (int64_t(1) << a.tw4_shift) - 1;
+    return cmul(__ldg(lo + (m & mask)), __ldg(hi + (m >> a.tw4_shift)));
+}
+
+// ------------------------------------------------------------------ passes
+// Persistent kernels: one CTA per SM loops over rows (column tiles); block
+// twiddles are copied to shared memory once per CTA, four-step twiddles of a
+// row (tile) are factored into 64 + len/64 entries built once per row (tile).
+// CHIRP: transfer function in the factored chirp form (two-level plans), else
+// the per-sample formula (single-level plans).
+template <typename Real, int LOG_L2, int E, bool CHIRP>
+__global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel(PassArgs a) {
+    using B = Block<Real, LOG_L2, 1, E>;
+    using Cx = typename B::Cx;
+    constexpr int L = B::L;
+    constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Cx *sm = reinterpret_cast<Cx *>(smraw);
+    Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
+    Cx *vec = tw + B::TW;  // per-row four-step factors: [0,64) low, [64, NV) high
+    constexpr int NQ = (L >> 6) > 1 ? (L >> 6) : 2;  // k2s >> 6 spans [-NQ/2, NQ/2)
+    Cx *chp = vec + NV;    // per-row chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
+    const int tp = threadIdx.x;
+    const int flags = a.flags;
+    const int64_t rows = a.n >> LOG_L2;
+    B::load_twiddles(tw, static_cast<const Cx *>(a.tw_row));
+    __syncthreads();
+    const int64_t nmask = a.n - 1;
+    const double inv_n = a.pr.fac;
+
+    for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int64_t k1 = digitrev_rt(row, a.log_n1);
+        if (CHIRP && a.pr.has_h) {
+            // phase of row k1: G k1^2 + g1 k2s with g1 = 2 N1 G k1 (turns);
+            // P[a] = A exp(2 pi i (G k1^2 + g1 a)), Q[b] = exp(2 pi i 64 g1 b)
+            const double n1 = double(int64_t(1) << a.log_n1);
+            const double gk = frac_dd(a.pr.g_hi, a.pr.g_lo, double(k1 * k1));
+            const double g1h = 2.0 * n1 * a.pr.g_hi, g1l = 2.0 * n1 * a.pr.g_lo;
+            for (int idx = tp; idx < 64 + NQ; idx += B::NT) {
+                double2 w;
+                if (idx < 64) {
+                    w = cmul(a.pr.A, cis_turns(gk + frac_dd(g1h, g1l, double(k1 * idx))));
+                } else {
+                    const int64_t b = int64_t(idx - 64) - NQ / 2;
+                    w = cis_turns(frac_dd(g1h, g1l, double(k1 * 64 * b)));
+                }
+                chp[idx] = cvt(w, Cx{});
+            }
+        }
+        if (flags & PF_TW) {
+            // conj(W_N^{n2 k1}) / N = conj(A[n2 & 63]) * conj(B[n2 >> 6]) / N
+            for (int idx = tp; idx < NV; idx += B::NT) {
+                const int64_t m = ((idx < 64 ? int64_t(idx) : int64_t(idx - 64) << 6) * k1) & nmask;
+                double2 w = w4(a, m);
+                w = make_double2(w.x, -w.y);
+                if (idx >= 64) w = make_double2(w.x * inv_n, w.y * inv_n);
+                vec[idx] = cvt(w, Cx{});
+            }
+        }
+        if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
+        const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + (row << LOG_L2);
+        Cx *__restrict__ gout = static_cast<Cx *>(a.out) + (row << LOG_L2);
+        Cx v[E];
+        if (!(flags & PF_SPEC_IN)) {
+#pragma unroll
+            for (int r = 0; r < E; ++r) v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[B::first_pos(tp, r)];
+            if (flags & PF_TRANS) {
+#pragma unroll
+                for (int r = 0; r < E; ++r) v[r] = apply_trans(a.tr, (row << LOG_L2) + B::first_pos(tp, r), v[r]);
+            }
+            if (flags & PF_FWD) B::forward(sm, tp, v, tw);
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r) v[r] = gin[B::last_pos(tp, r)];
+        }
+
+        if constexpr (CHIRP) {
+          if (a.pr.has_h) {
+            // H = P[k2s & 63] * Q[k2s >> 6] * h3[r][tp], zero in the cutoff range
+            const int half2 = 1 << (LOG_L2 - 1);
+            const Cx *h3 = static_cast<const Cx *>(a.pr.h3);
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const int k2 = B::last_freq(tp, r);
+                const int64_t k = k1 + (int64_t(k2) << a.log_n1);
+                const int k2s = k2 >= half2 ? k2 - 2 * half2 : k2;
+                const Cx h = cmul(cmul(chp[k2s & 63], chp[64 + (k2s >> 6) + NQ / 2]), __ldg(h3 + r * B::T + tp));
+                v[r] = (a.pr.has_cut && k >= a.pr.cut_lo && k < a.pr.cut_hi) ? Cx{} : cmul(v[r], h);
+            }
+          } else if (a.pr.has_cut) {
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const int64_t k = k1 + (int64_t(B::last_freq(tp, r)) << a.log_n1);
+                if (k >= a.pr.cut_lo && k < a.pr.cut_hi) v[r] = Cx{};
+            }
+          }
+        } else if (a.pr.has_h || a.pr.has_cut) {
+            const int64_t half2 = int64_t(1) << (LOG_L2 - 1);
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const int64_t k2 = B::last_freq(tp, r);
+                const int64_t k = k1 + (k2 << a.log_n1);
+                const int64_t k2s = k2 >= half2 ? k2 - 2 * half2 : k2;
+                const int64_t ks = k1 + k2s * (int64_t(1) << a.log_n1);
+                v[r] = prop_apply(a.pr, k, ks, v[r]);
+            }
+        }
+
+        if (flags & PF_INV) {
+            B::inverse(sm, tp, v, tw);
+            if (flags & PF_TW) {
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int n2 = B::first_pos(tp, r);
+                    v[r] = cmul(cmul(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                }
+            } else if (flags & PF_SCALE) {
+                const Real f = Real(a.pr.fac);
+#pragma unroll
+                for (int r = 0; r < E; ++r) v[r] = cscale(v[r], f);
+            }
+#pragma unroll
+            for (int r = 0; r < E; ++r) gout[B::first_pos(tp, r)] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r) gout[B::last_pos(tp, r)] = v[r];
+        }
+        __syncthreads();
+    }
+}
+
+template <typename Real, int LOG_L1, int C, int E>
+__global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(PassArgs a) {
+    using B = Block<Real, LOG_L1, C, E>;
+    using Cx = typename B::Cx;
+    constexpr int L = B::L;
+    constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int t = threadIdx.x;
+    const int c = t % C;
+    const int tp = t / C;
+    Cx *sm = reinterpret_cast<Cx *>(smraw) + c * B::PITCH;
+    Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
+    Cx *vec = tw + B::TW;  // per-column four-step factors, NV per column
+    const int log_n2 = a.log_n2;
+    const int flags = a.flags;
+    const int64_t tiles = (int64_t(1) << log_n2) / C;
+    const int64_t nmask = a.n - 1;
+    B::load_twiddles(tw, static_cast<const Cx *>(a.tw_col));
+    __syncthreads();
+
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int64_t col0 = tile * C;
+        const int64_t col = col0 + c;
+        if (flags & PF_TW) {
+            // W_N^{n2 k1} = A[k1 & 63] * B[k1 >> 6] for each of the C columns
+            for (int idx = t; idx < C * NV; idx += B::NT) {
+                const int cc = idx / NV, e = idx % NV;
+                const int64_t m = ((e < 64 ? int64_t(e) : int64_t(e - 64) << 6) * (col0 + cc)) & nmask;
+                vec[idx] = cvt(w4(a, m), Cx{});
+            }
+        }
+        const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + col;
+        Cx *__restrict__ gout = static_cast<Cx *>(a.out) + col;
+        Cx v[E];
+        if (flags & PF_INV) {
+#pragma unroll
+            for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
+            B::inverse(sm, tp, v, tw);
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r)
+                v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[int64_t(B::first_pos(tp, r)) << log_n2];
+        }
+        if (flags & PF_TRANS) {
+#pragma unroll
+            for (int r = 0; r < E; ++r)
+                v[r] = apply_trans(a.tr, (int64_t(B::first_pos(tp, r)) << log_n2) + col, v[r]);
+        }
+        if (flags & PF_FWD) {
+            B::forward(sm, tp, v, tw);
+            if (flags & PF_TW) {
+                const Cx *vc = vec + c * NV;
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int k1 = B::last_freq(tp, r);
+                    v[r] = cmul(v[r], cmul(vc[k1 & 63], vc[64 + (k1 >> 6)]));
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < E; ++r) gout[int64_t(B::last_pos(tp, r)) << log_n2] = v[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < E; ++r) gout[int64_t(B::first_pos(tp, r)) << log_n2] = v[r];
+        }
+        __syncthreads();
+    }
+}
+
+// exp(2 pi i G N1^2 k2s^2) for every register (r, tp) of the row kernel
+// Block<Real, LOG_L2, 1, E>, stored at r * T + tp.
+template <typename Real, int LOG_L2, int E>
+__global__ void chirp_table_kernel(typename CxT<Real>::T *__restrict__ out, double g3_hi, double g3_lo) {
+    using B = Block<Real, LOG_L2, 1, E>;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= B::L) return;
+    const int r = idx / B::T, tp = idx % B::T;
+    const int half2 = 1 << (LOG_L2 - 1);
+    const int k2 = B::last_freq(tp, r);
+    const double k2s = double(k2 >= half2 ? k2 - 2 * half2 : k2);
+    out[idx] = cvt(cis_turns(frac_dd(g3_hi, g3_lo, k2s * k2s)), typename CxT<Real>::T{});
+}
+
+void count_launch();
+
+template <typename K> static cudaError_t prep(K kernel, size_t smem) {
+    if (smem > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    return cudaSuccess;
+}
+
+// persistent grid: as many CTAs as fit on the device at once, capped by the work
+template <typename K> static int64_t resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    return int64_t(sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+}
+
+template <int L> constexpr int n_vec() { return 64 + ((L >> 6) > 0 ? (L >> 6) : 1); }
+template <int L> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) : 2); }
+
+template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
+    using B = Block<Real, LG, 1, E>;
+    auto k = row_pass_kernel<Real, LG, E, CH>;
+    const size_t smem = B::SMEM + size_t(n_vec<B::L>() + n_chirp<B::L>()) * sizeof(typename B::Cx);
+    static cudaError_t attr = prep(k, smem);
+    if (attr != cudaSuccess) return attr;
+    static int64_t cap = resident_ctas(k, B::NT, smem);
+    const int64_t rows = a.n >> LG;
+    k<<<dim3(unsigned(rows < cap ? rows : cap)), dim3(B::NT), smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
+    using B = Block<Real, LG, C, E>;
+    auto k = col_pass_kernel<Real, LG, C, E>;
+    const size_t smem = B::SMEM + size_t(C) * n_vec<B::L>() * sizeof(typename B::Cx);
+    static cudaError_t attr = prep(k, smem);
+    if (attr != cudaSuccess) return attr;
+    static int64_t cap = resident_ctas(k, B::NT, smem);
+    const int64_t tiles = (int64_t(1) << a.log_n2) / C;
+    k<<<dim3(unsigned(tiles < cap ? tiles : cap)), dim3(B::NT), smem, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename Real, int LG, int E> static cudaError_t chirp_impl(void *out, double hi, double lo, cudaStream_t s) {
+    chirp_table_kernel<Real, LG, E><<<((1 << LG) + 255) / 256, 256, 0, s>>>(
+        static_cast<typename CxT<Real>::T *>(out), hi, lo);
+    count_launch();
+    return cudaGetLastError();
+}
+}  // namespace rsw

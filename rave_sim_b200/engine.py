@@ -347,6 +347,14 @@ class Simulation:
         L.check(self._lib.rsw_sim_read(self._h, out.ctypes.data_as(L._DP), _stream_ptr()))
         return out
 
+    def detected_device(self, out=None):
+        """The FP64 accumulator copied into a CUDA tensor (asynchronous)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.nr_phase_steps, self.n_pix), dtype=torch.float64, device="cuda")
+        L.check(self._lib.rsw_sim_read_device(self._h, C.cast(_dptr(out), L._DP), _stream_ptr()))
+        return out
+
     def accumulator(self):
         """Device pointer of the FP64 accumulator."""
         p = L._DP()

@@ -393,6 +393,13 @@ def main():
     units["cut_zero_first"] = np.array([z[0] if len(z) else -1 for *_, z in cut])
     np.savez_compressed(HERE / "units.npz", **units)
 
+    # ---- Al attenuation for the bremsstrahlung spectrum weights ------------
+    # mu_Al(E) = 1/atlen from the reference's material lookup
+    # (nist_lookup/nist_lookup/xraydb_plugin.py:134-181), density 2.70 g/cm^3
+    energies = np.arange(10000.0, 80001.0, 500.0)
+    mu = np.array([1.0 / optical_element.xray_delta_beta("Al", 2.70, float(e))[2] for e in energies])
+    np.savez_compressed(HERE / "al_attenuation.npz", energy_ev=energies, mu_per_cm=mu)
+
     # ---- TestSnapshot (big-wave/test.py:853-960) --------------------------
     with tempfile.TemporaryDirectory() as td:
         td = Path(td)

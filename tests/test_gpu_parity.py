@@ -3,7 +3,10 @@ golden vectors. Every call goes through the C ABI (librsw.so via ctypes).
 
 Tolerances:
   c16 (FP64) detector output: rel-L2 <= 1e-10 vs the reference's FP64 output;
-  c16 FFT / propagate: rel-L2 <= 1e-12;
+  c16 FFT: rel-L2 <= 1e-12; c16 propagate on white-spectrum random fields:
+      rel-L2 <= 1e-10 vs the reference's rounded phase and <= 1e-13 vs the
+      exactly evaluated phase (the engine evaluates c*fx^2 without the
+      reference's intermediate roundings on two-level plans);
   c8  (FP32 fields, FP64 phases and sums) detector output: rel-L2 <= 1e-5
       vs the FP64 reference, FFT rel-L2 <= 2e-6.
 """
@@ -84,9 +87,13 @@ def test_propagate_matches_oracle(dt, logn, skip):
     Ud = to_dev(U0.astype(np.complex128 if dt == "c16" else np.complex64)) if skip else \
         torch.empty(n, dtype=p.dtype, device=DEV)
     p.propagate(ud, Ud, dx=dx, wl=wl, dz=0.0818, cutoff_freq=cut, skip_fft=skip)
-    tol = 1e-12 if dt == "c16" else 1e-5
+    tol = 1e-10 if dt == "c16" else 1e-5
     assert rel_l2(ud.cpu().numpy(), u_ref) < tol
     assert rel_l2(Ud.cpu().numpy(), U_ref) < tol
+    if dt == "c16":
+        u_ex, U_ex = bw.propagate(u, U0, sim, 0.0818, cut, skip_fft=skip, exact_phase=True)
+        exact = p.info()["log_rows"] > 0  # two-level plans use the exact phase
+        assert rel_l2(ud.cpu().numpy(), u_ex if exact else u_ref) < 1e-13
     if not skip:
         ud2 = to_dev(u.astype(np.complex128 if dt == "c16" else np.complex64))
         p.propagate(ud2, None, dx=dx, wl=wl, dz=0.0818, cutoff_freq=cut)
