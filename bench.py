@@ -209,8 +209,11 @@ def main():
     lib = rsw.load_library()
     n = 1 << args.logn
     case = workloads.talbot_lau(n=n, dtype=args.dtype)
+    from rave_sim_b200.sharding import reduce_detector, shard_sources
+
     all_e, all_w = workloads.config2_energies(args.energies * ws)
-    my_e, my_w = all_e[rank::ws], all_w[rank::ws]
+    mine = shard_sources([1.0] * len(all_e), ws)[rank]  # equal cost: same N and schedule per energy
+    my_e, my_w = all_e[mine], all_w[mine]
     sim = rsw.Simulation(case, dtype=args.dtype)
     acc = torch.zeros((sim.nr_phase_steps, sim.n_pix), dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
@@ -221,10 +224,7 @@ def main():
             sim.run_source(energy=float(e), db_table=workloads.db_table(float(e)), source=source,
                            weight=float(w), field=field)
         sim.detected_device(acc)
-        if ws > 1:
-            import torch.distributed as dist
-
-            dist.all_reduce(acc)
+        reduce_detector(acc)
 
     def barrier():
         torch.cuda.synchronize()

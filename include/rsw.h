@@ -190,6 +190,7 @@ typedef struct {
     const double *deltabeta;
     int64_t n_deltabeta;         /* number of {delta, beta} pairs                       */
     double weight;               /* accumulation weight of this source's detector output */
+    double wavelength_m;         /* > 0: use this wavelength instead of deriving it from energy_ev */
 } rsw_source_run;
 
 rsw_status rsw_sim_create(rsw_sim *out, const rsw_sim_desc *desc);

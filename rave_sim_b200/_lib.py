@@ -83,6 +83,7 @@ class SourceRun(C.Structure):
         ("deltabeta", C.POINTER(C.c_double)),
         ("n_deltabeta", C.c_int64),
         ("weight", C.c_double),
+        ("wavelength_m", C.c_double),
     ]
 
 

@@ -1220,13 +1220,14 @@ rsw_status rsw_sim_timing(rsw_sim S, int kind, double *ms, int64_t *launches) {
 
 rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
     if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
-    if (!(run->energy_ev > 0)) return fail(RSW_ERR_INVALID, "energy must be positive");
+    if (!(run->energy_ev > 0) && !(run->wavelength_m > 0))
+        return fail(RSW_ERR_INVALID, "energy or wavelength must be positive");
     ++g_api_calls;
     Runner R;
     R.S = S;
     R.P = S->plan;
     R.st = (cudaStream_t)stream;
-    R.wl = wavelength(run->energy_ev);
+    R.wl = run->wavelength_m > 0 ? run->wavelength_m : wavelength(run->energy_ev);
     for (double a : S->cutoff_angles) R.cut.push_back(std::sin(a) / R.wl);
     // deltabeta per element
     int64_t k = 0;

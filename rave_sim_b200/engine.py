@@ -298,7 +298,7 @@ class Simulation:
         L.check(self._lib.rsw_sim_reset(self._h, _stream_ptr()))
 
     def run_source(self, *, energy: float, db_table, source: dict, weight: float = 1.0,
-                   field=None):
+                   field=None, wavelength: Optional[float] = None):
         """Run one source (big-wave wavesim.run_simulation) and add
         ``weight * detected`` to the device accumulator.
 
@@ -339,6 +339,7 @@ class Simulation:
         run.deltabeta = db.view(np.float64).ctypes.data_as(L._DP) if db.size else None
         run.n_deltabeta = db.size
         run.weight = float(weight)
+        run.wavelength_m = float(wavelength) if wavelength is not None else 0.0
         L.check(self._lib.rsw_sim_run(self._h, C.byref(src), C.byref(run), _stream_ptr()))
 
     def detected(self) -> np.ndarray:
