@@ -77,6 +77,23 @@ rsw_status rsw_plan_info(rsw_plan plan, int64_t *n, int *dtype, int *log_rows,
 rsw_status rsw_fft_forward(rsw_plan plan, const void *d_in, void *d_out, void *stream);
 rsw_status rsw_fft_inverse(rsw_plan plan, const void *d_in, void *d_out, void *stream);
 
+/* No counterpart in the reference. The natural-order forward FFT of
+ * rsw_fft_forward (same result) for callers that cannot allocate device
+ * memory where they need it: a process whose free device memory is owned by
+ * another allocator (a framework's caching allocator, so a raw cudaMalloc
+ * fails or fragments it), or a latency-sensitive loop that must not pay the
+ * device-wide synchronisation of cudaFree. It needs no plan and allocates
+ * nothing: its scratch is a fixed 1.5 MiB array in the library's device
+ * image (held by every GPU that loads the library until exit), so n is
+ * limited to RSW_NOALLOC_MAX_N samples; larger n returns RSW_ERR_INVALID.
+ * The first call on each device (with that device current) looks up the
+ * array's device address; make that call before any stream capture. All
+ * calls share the array and it keeps the last call's contents (tables are
+ * rebuilt when n or dtype changes); calls that overlap on the GPU race and
+ * must be serialised by the caller. in == out is allowed. */
+#define RSW_NOALLOC_MAX_N 65536
+rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int64_t n, int dtype, void *stream);
+
 /* big-wave propagation.propagate (big-wave/propagation.py:100-138) and
  * fast-wave propagate<S> (fast-wave/src/simulation.cpp:34-40): u <- iFFT(H * FFT(u))
  * with H the Fresnel transfer function of distance dz and the big-wave frequency

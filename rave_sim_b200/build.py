@@ -28,7 +28,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
 ]
 
-SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_kernels.cu", "rsw_host.cpp"]
+SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_kernels.cu", "rsw_noalloc.cu", "rsw_host.cpp"]
 HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh"]
 
 

@@ -60,6 +60,13 @@ static rsw_status fail(rsw_status st, const char *fmt, ...) {
     return st;
 }
 
+namespace rsw {
+rsw_status set_error(rsw_status st, const char *msg) {
+    t_last_error = msg;
+    return st;
+}
+}  // namespace rsw
+
 #define CU(call)                                                                               \
     do {                                                                                       \
         cudaError_t e_ = (call);                                                               \
