@@ -375,8 +375,14 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *l2)
         *l1 = 0;
         *l2 = lg;
     } else {
-        int a = std::min(col_max, lg / 2);
+        // prefer columns of at most 2^11 (the 2^12 c64 column kernel runs 1024
+        // threads at 64 registers and spills); rows take the rest
+        int a = std::min(std::min(col_max, 11), lg / 2);
         int b = lg - a;
+        if (b > row_max) {
+            a = lg - row_max;
+            b = row_max;
+        }
         if (b < 7) {  // rows of two-level plans hold at least 2^7 samples
             b = 7;
             a = lg - b;

@@ -88,8 +88,8 @@ __device__ __forceinline__ double sample_row_x(const TransArgs &t, int64_t j) {
     return __dsub_rn(__dadd_rn(__dmul_rn(double(j), t.psx), t.sample_xpos), t.sample_hw);
 }
 
-static __device__ __noinline__ double2 sample_interp(const TransArgs &t, int64_t j, int m0, int m1, double x,
-                                              double xj);
+static __device__ __noinline__ double2 sample_interp(const double2 *mat_db, double psx, double xpos, double hw,
+                                                     double y, int64_t j, int m0, int m1, double x, double xj);
 
 // Sample row factor at sample n: exp(i y * np.interp(x, row_x, row_db, 0, 0))
 // (big-wave/optical_element.py:452-472). Returns false for vacuum (factor 1).
@@ -119,25 +119,27 @@ __device__ __forceinline__ bool sample_factor(const TransArgs &t, int64_t n, dou
         *f = t.mat_factor[m0];
         return true;
     }
-    *f = sample_interp(t, j, m0, m1, x, xj);
+    // scalars by value: a reference to the kernel parameter would force it into local memory
+    *f = sample_interp(t.mat_db, t.psx, t.sample_xpos, t.sample_hw, t.sample_y, j, m0, m1, x, xj);
     return true;
 }
 
 // Interpolated delta+i*beta between two different pixels and its factor
 // exp(i y db); kept out of line (only samples at material boundaries get here).
-static __device__ __noinline__ double2 sample_interp(const TransArgs &t, int64_t j, int m0, int m1, double x,
-                                              double xj) {
-    const double2 d0 = t.mat_db[m0], d1 = t.mat_db[m1];
-    const double dxp = __dsub_rn(sample_row_x(t, j + 1), xj);
+static __device__ __noinline__ double2 sample_interp(const double2 *mat_db, double psx, double xpos, double hw,
+                                                     double y, int64_t j, int m0, int m1, double x, double xj) {
+    const double2 d0 = mat_db[m0], d1 = mat_db[m1];
+    const double xj1 = __dsub_rn(__dadd_rn(__dmul_rn(double(j + 1), psx), xpos), hw);
+    const double dxp = __dsub_rn(xj1, xj);
     const double sre = __ddiv_rn(__dsub_rn(d1.x, d0.x), dxp);
     const double sim = __ddiv_rn(__dsub_rn(d1.y, d0.y), dxp);
     const double xr = __dsub_rn(x, xj);
     const double dre = __dadd_rn(__dmul_rn(sre, xr), d0.x);
     const double dim = __dadd_rn(__dmul_rn(sim, xr), d0.y);
     // exp((0, y) * (dre, dim)) = exp(-y*dim) * (cos(y*dre), sin(y*dre))
-    const double amp = exp(-__dmul_rn(t.sample_y, dim));
+    const double amp = exp(-__dmul_rn(y, dim));
     double s, c;
-    sincos(__dmul_rn(t.sample_y, dre), &s, &c);
+    sincos(__dmul_rn(y, dre), &s, &c);
     return make_double2(amp * c, amp * s);
 }
 
@@ -360,6 +362,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     using Cx = typename B::Cx;
     constexpr int L = B::L;
     constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
+    constexpr int NVP = NV | 1;  // odd per-column stride: the C columns' factors fall in different banks
     extern __shared__ __align__(16) unsigned char smraw[];
     const int t = threadIdx.x;
     const int c = t % C;
@@ -382,7 +385,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
             for (int idx = t; idx < C * NV; idx += B::NT) {
                 const int cc = idx / NV, e = idx % NV;
                 const int64_t m = ((e < 64 ? int64_t(e) : int64_t(e - 64) << 6) * (col0 + cc)) & nmask;
-                vec[idx] = cvt(w4(a, m), Cx{});
+                vec[cc * NVP + e] = cvt(w4(a, m), Cx{});
             }
         }
         const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + col;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
-                const Cx *vc = vec + c * NV;
+                const Cx *vc = vec + c * NVP;
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int k1 = B::last_freq(tp, r);
@@ -471,7 +474,7 @@ template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(con
 template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
     auto k = col_pass_kernel<Real, LG, C, E>;
-    const size_t smem = B::SMEM + size_t(C) * n_vec<B::L>() * sizeof(typename B::Cx);
+    const size_t smem = B::SMEM + size_t(C) * (n_vec<B::L>() | 1) * sizeof(typename B::Cx);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
