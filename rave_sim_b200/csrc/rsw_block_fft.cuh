@@ -1,18 +1,23 @@
 // Block FFT building blocks for the split-step passes (sm_100a).
 //
 // A "block" transforms C independent sequences of length L = 2^LOG_L held by
-// one CTA. Each thread owns E = 16 elements in registers; stages are radix-16
-// (the first stage takes the remaining radix 2/4/8/16). Forward stages are
-// decimation in frequency: natural order in, digit-reversed order out.
-// Inverse stages are the exact mirror (decimation in time): digit-reversed
-// in, natural out, so a forward/inverse pair needs no reordering and the
-// propagator is applied to the digit-reversed spectrum in registers.
+// one CTA. Each thread owns E = 16 (or 32) elements in registers; stages are
+// radix-16, the last one takes the remaining radix 2/4/8/16 (rsw_stages.h).
+// Forward stages are decimation in frequency: natural order in,
+// digit-reversed order out. Inverse stages are the exact mirror (decimation
+// in time): digit-reversed in, natural out, so a forward/inverse pair needs
+// no reordering and the propagator is applied to the digit-reversed spectrum
+// in registers.
 //
 // Stage s has radix R_s = 2^lr(s) and stride S_s = 2^ls(s). Butterfly beta
-// (beta = tp + T*i) of stage s touches positions
+// of stage s touches positions
 //     (beta >> ls) * R*S + (beta & (S-1)) + q*S,   q = 0..R-1
-// and is done by one thread, which reads and writes the same positions, so
-// stages exchange data through shared memory with one barrier each.
+// and is done by one thread, which reads and writes the same positions.
+// Only the exchange between stages 0 and 1 spans the whole sequence; every
+// later exchange stays inside a block of stage s, owned by a contiguous
+// group of threads (Radix::beta), and is ordered by a barrier of that group
+// alone: a warp or less for all but the longest blocks, so warps run through
+// the inner stages without waiting for each other.
 //
 // Inside a butterfly the radix-R DFT is a radix-2 network in registers: the
 // forward network takes natural order and leaves bit-reversed order (register
@@ -20,7 +25,7 @@
 // leaves natural order, so no register permutation is ever needed.
 //
 // Twiddles W_{RS}^{jq} of stage s live in shared memory, loaded once per CTA:
-// a direct table [(q-1)*S + j] for strides S <= 256, otherwise two factors
+// a direct table [(q-1)*S + j] for strides S <= 128, otherwise two factors
 // W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64 entries per q.
 // Shared memory holds the C sequences with one pad element per 16 (phys(p))
 // and a per-sequence pitch chosen so that the accesses of one wavefront hit
@@ -30,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <type_traits>
+
+#include "rsw_stages.h"
 
 namespace rsw {
 
@@ -118,55 +125,23 @@ template <int LOG_L, int E_ = 16> struct Radix {
     static constexpr int L = 1 << LOG_L;
     static constexpr int E = E_;
     static constexpr int T = L / E;  // threads per sequence
-    static constexpr int NS = (LOG_L + 3) / 4;
-    static constexpr int LR0 = LOG_L - 4 * (NS - 1);
-    __host__ __device__ static constexpr int lr(int s) { return s == 0 ? LR0 : 4; }
-    __host__ __device__ static constexpr int ls(int s) { return LOG_L - LR0 - 4 * s; }
-    __host__ __device__ static constexpr bool direct(int s) { return ls(s) <= 8; }
-    __host__ __device__ static constexpr int tw_entries(int s) {
-        return s >= NS - 1 ? 0
-               : direct(s) ? ((1 << lr(s)) - 1) << ls(s)
-                           : ((1 << lr(s)) - 1) * (64 + (1 << (ls(s) - 6)));
-    }
-    __host__ __device__ static constexpr int twoff(int s) {
-        int o = 0;
-        for (int t = 0; t < s; ++t) o += tw_entries(t);
-        return o;
-    }
+    static constexpr int NS = stage_count(LOG_L);
+    __host__ __device__ static constexpr int lr(int s) { return stage_lr(LOG_L, s); }
+    __host__ __device__ static constexpr int ls(int s) { return stage_ls(LOG_L, s); }
+    __host__ __device__ static constexpr bool direct(int s) { return stage_direct(LOG_L, s); }
+    __host__ __device__ static constexpr int twoff(int s) { return stage_tw_offset(LOG_L, s); }
     static constexpr int TW = twoff(NS - 1) > 0 ? twoff(NS - 1) : 1;
+    // butterflies per thread in stage s
+    __host__ __device__ static constexpr int M(int s) { return E >> lr(s); }
+    // Butterfly i of thread tp in stage s. Stage 0 strides by T (consecutive
+    // threads touch consecutive positions: coalesced global access); later
+    // stages give each thread M consecutive butterflies, so that every block
+    // of stage s (R_s * S_s positions) belongs to a contiguous, aligned range
+    // of R_s * S_s / E threads and the exchange after stage s stays inside it.
+    __host__ __device__ static constexpr int beta(int s, int tp, int i) { return s == 0 ? tp + T * i : tp * M(s) + i; }
+    // threads of one sequence that exchange data between stages s and s + 1
+    __host__ __device__ static constexpr int group(int s) { return s == 0 ? T : (1 << (lr(s) + ls(s))) / E; }
 };
-
-// Digit reversal of a block position for a block of length 2^log_l (runtime
-// variant, used for row indices of the column level).
-__host__ __device__ inline int64_t digitrev_rt(int64_t p, int log_l) {
-    if (log_l <= 0) return 0;
-    const int ns = (log_l + 3) / 4;
-    const int lr0 = log_l - 4 * (ns - 1);
-    int64_t f = 0;
-    int sh = 0;
-    for (int s = 0; s < ns; ++s) {
-        const int lr = s == 0 ? lr0 : 4;
-        const int ls = log_l - lr0 - 4 * s;
-        f |= ((p >> ls) & ((1 << lr) - 1)) << sh;
-        sh += lr;
-    }
-    return f;
-}
-// Inverse of digitrev_rt: frequency index -> block position.
-__host__ __device__ inline int64_t digitpos_rt(int64_t f, int log_l) {
-    if (log_l <= 0) return 0;
-    const int ns = (log_l + 3) / 4;
-    const int lr0 = log_l - 4 * (ns - 1);
-    int64_t p = 0;
-    int sh = 0;
-    for (int s = 0; s < ns; ++s) {
-        const int lr = s == 0 ? lr0 : 4;
-        const int ls = log_l - lr0 - 4 * s;
-        p |= ((f >> sh) & ((1 << lr) - 1)) << ls;
-        sh += lr;
-    }
-    return p;
-}
 
 template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG_L, E_> {
     using Rx = Radix<LOG_L, E_>;
@@ -188,7 +163,7 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
 
     template <int s> __device__ static __forceinline__ int pos(int tp, int i, int q) {
         constexpr int LRS = Rx::lr(s), LSS = Rx::ls(s);
-        const int beta = tp + T * i;
+        const int beta = Rx::beta(s, tp, i);
         const int j = beta & ((1 << LSS) - 1);
         const int b = beta >> LSS;
         return (b << (LRS + LSS)) + j + (q << LSS);
@@ -236,7 +211,7 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
         for (int i = 0; i < E / R; ++i) {
             net_dif<R, -1>(v + i * R);
             if constexpr (s < NS - 1) {
-                const int j = (tp + T * i) & ((1 << LSS) - 1);
+                const int j = Rx::beta(s, tp, i) & ((1 << LSS) - 1);
 #pragma unroll
                 for (int q = 1; q < R; ++q) {
                     Cx &x = v[reg<s, true>(i, q)];
@@ -252,7 +227,7 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
 #pragma unroll
         for (int i = 0; i < E / R; ++i) {
             if constexpr (s < NS - 1) {
-                const int j = (tp + T * i) & ((1 << LSS) - 1);
+                const int j = Rx::beta(s, tp, i) & ((1 << LSS) - 1);
 #pragma unroll
                 for (int q = 1; q < R; ++q) {
                     Cx &x = v[reg<s, true>(i, q)];
@@ -263,13 +238,33 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
         }
     }
 
+    // Barrier of the exchange between stages s and s + 1 (either direction).
+    // The exchanging threads form aligned groups of Rx::group(s) * C
+    // consecutive threads (threads are numbered tp * C + c): one warp or less
+    // synchronises with __syncwarp, larger groups with a named barrier of
+    // their own, the whole CTA with __syncthreads. Each position is written
+    // in a stage only by the thread that read it in that stage, so one
+    // barrier per exchange orders every access.
+    template <int s> __device__ static __forceinline__ void exchange_sync() {
+        constexpr int G = Rx::group(s) * C;
+        if constexpr (G >= NT) {
+            __syncthreads();
+        } else if constexpr (G <= 32) {
+            __syncwarp();
+        } else if constexpr (NT / G <= 15) {
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + int(threadIdx.x) / G), "r"(G) : "memory");
+        } else {
+            __syncthreads();
+        }
+    }
+
     // Full forward transform from stage-0 positions (natural layout) to
     // last-stage positions (bit-reversed layout) in registers.
     template <int s = 0> __device__ static __forceinline__ void forward(Cx *sm, int tp, Cx *v, const Cx *tw) {
         dif<s>(tp, v, tw);
         if constexpr (s < NS - 1) {
             st<s, true>(sm, tp, v);
-            __syncthreads();
+            exchange_sync<s>();
             ld<s + 1, false>(sm, tp, v);
             forward<s + 1>(sm, tp, v, tw);
         }
@@ -280,7 +275,7 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
         dit<s>(tp, v, tw);
         if constexpr (s > 0) {
             st<s, false>(sm, tp, v);
-            __syncthreads();
+            exchange_sync<s - 1>();
             ld<s - 1, true>(sm, tp, v);
             inverse<s - 1>(sm, tp, v, tw);
         }
@@ -296,10 +291,14 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
         constexpr int LRL = Rx::lr(NS - 1);
         return pos<NS - 1>(tp, r / RL, brev_bits(r % RL, LRL));
     }
-    // digit-reversed frequency index of last_pos(tp, r)
-    __device__ static __forceinline__ int last_freq(int tp, int r) {
-        return int(digitrev_rt(last_pos(tp, r), LOG_L));
-    }
+    // Frequency index of last_pos(tp, r). The last stage gives thread tp the
+    // E consecutive positions tp*E + last_off(r), so the frequency splits into
+    // a per-thread part and a compile-time part with disjoint bits:
+    // last_freq(tp, r) == freq_base(tp) | freq_off(r).
+    static constexpr int last_off(int r) { return (r / RL) * RL + brev_bits(r % RL, Rx::lr(NS - 1)); }
+    static constexpr int freq_off(int r) { return digitrev_c(last_off(r), LOG_L); }
+    __device__ static __forceinline__ int freq_base(int tp) { return digitrev_c(tp * E, LOG_L); }
+    __device__ static __forceinline__ int last_freq(int tp, int r) { return freq_base(tp) | freq_off(r); }
 
     // copy the block's twiddle tables (global, host-built layout) into shared memory
     __device__ static __forceinline__ void load_twiddles(Cx *tw_sm, const Cx *__restrict__ tw_g) {

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "rsw_internal.h"
+#include "rsw_stages.h"
 
 namespace rsw {
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
@@ -320,27 +321,17 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
     v.push_back(T(c.imag()));
 }
 
-// Block twiddle tables of a block of length 2^log_l, in the shared-memory
-// layout of Radix<LOG_L>: per stage s (all but the last), W_{RS}^{jq} for
-// q = 1..R-1, j < S, either direct [(q-1)*S + j] (S <= 256) or factored as
-// W^{(j & 63) q} [(q-1)*64 + (j & 63)] and W^{64 (j >> 6) q} [(R-1)*64 + (q-1)*(S/64) + (j >> 6)].
+// Block twiddle tables of a block of length 2^log_l in the shared-memory
+// layout of the block FFT (rsw_stages.h): stages in order, entry k of stage s
+// is W_{RS}^m with (m, RS) from stage_tw_entry.
 template <typename T> static std::vector<T> block_twiddles(int log_l) {
     std::vector<T> v;
     if (log_l >= 4) {
-        const int ns = (log_l + 3) / 4;
-        const int lr0 = log_l - 4 * (ns - 1);
-        for (int s = 0; s < ns - 1; ++s) {
-            const int lr = s == 0 ? lr0 : 4;
-            const int ls = log_l - lr0 - 4 * s;
-            const int64_t R = int64_t(1) << lr, S = int64_t(1) << ls;
-            if (ls <= 8) {
-                for (int64_t q = 1; q < R; ++q)
-                    for (int64_t j = 0; j < S; ++j) push_c(v, twiddle(j * q, R * S));
-            } else {
-                for (int64_t q = 1; q < R; ++q)
-                    for (int64_t j = 0; j < 64; ++j) push_c(v, twiddle(j * q, R * S));
-                for (int64_t q = 1; q < R; ++q)
-                    for (int64_t j = 0; j < S / 64; ++j) push_c(v, twiddle(64 * j * q, R * S));
+        for (int s = 0; s < stage_count(log_l) - 1; ++s) {
+            for (int64_t k = 0; k < stage_tw_entries(log_l, s); ++k) {
+                int64_t m, mod;
+                stage_tw_entry(log_l, s, k, &m, &mod);
+                push_c(v, twiddle(m, mod));
             }
         }
     }

@@ -63,31 +63,18 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[1536 * 1024];
 namespace {
 
 // Block twiddles of a block of length 2^log_l into `out` in the layout of
-// Radix<LOG_L> (direct tables for strides <= 256, 64-factored otherwise);
-// W_M^m = exp(-2 pi i m / M) from sincospi of an exact argument.
+// the block FFT (rsw_stages.h); W_M^m = exp(-2 pi i m / M) from sincospi of
+// an exact argument.
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
-    const int ns = (log_l + 3) / 4;
-    const int lr0 = log_l - 4 * (ns - 1);
     int off = 0;
-    for (int s = 0; s < ns - 1; ++s) {
-        const int lr = s == 0 ? lr0 : 4;
-        const int ls = log_l - lr0 - 4 * s;
-        const int64_t R = int64_t(1) << lr, S = int64_t(1) << ls, M = R * S;
-        const bool direct = ls <= 8;
-        const int count = direct ? int((R - 1) * S) : int((R - 1) * (64 + S / 64));
+    for (int s = 0; s < stage_count(log_l) - 1; ++s) {
+        const int count = stage_tw_entries(log_l, s);
         for (int k = idx; k < count; k += stride) {
-            int64_t m;
-            if (direct) {
-                m = (k / S + 1) * (k % S);
-            } else if (k < (R - 1) * 64) {
-                m = (k / 64 + 1) * (k % 64);
-            } else {
-                const int kk = int(k - (R - 1) * 64);
-                m = (kk / (S / 64) + 1) * 64 * (kk % (S / 64));
-            }
+            int64_t m, mod;
+            stage_tw_entry(log_l, s, k, &m, &mod);
             double sn, cs;
-            sincospi(-2.0 * double(m % M) / double(M), &sn, &cs);
+            sincospi(-2.0 * double(m % mod) / double(mod), &sn, &cs);
             out[2 * (off + k)] = T(cs);
             out[2 * (off + k) + 1] = T(sn);
         }

@@ -229,6 +229,13 @@ __device__ __forceinline__ double2 w4(const PassArgs &a, int64_t m) {
     return cmul(__ldg(lo + (m & mask)), __ldg(hi + (m >> a.tw4_shift)));
 }
 
+// ceil(x / 2^log_n1) clamped to [0, l]: the first row frequency k2 with
+// k1 + k2 * 2^log_n1 >= k1 + x
+__device__ __forceinline__ int k2_bound(int64_t x, int log_n1, int l) {
+    const int64_t c = -((-x) >> log_n1);
+    return c < 0 ? 0 : (c > l ? l : int(c));
+}
+
 // ------------------------------------------------------------------ passes
 // Persistent kernels: one CTA per SM loops over rows (column tiles); block
 // twiddles are copied to shared memory once per CTA, four-step twiddles of a
@@ -244,9 +251,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
     extern __shared__ __align__(16) unsigned char smraw[];
     Cx *sm = reinterpret_cast<Cx *>(smraw);
     Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
-    Cx *vec = tw + B::TW;  // per-row four-step factors: [0,64) low, [64, NV) high
     constexpr int NQ = (L >> 6) > 1 ? (L >> 6) : 2;  // k2s >> 6 spans [-NQ/2, NQ/2)
-    Cx *chp = vec + NV;    // per-row chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
     const int tp = threadIdx.x;
     const int flags = a.flags;
     const int64_t rows = a.n >> LOG_L2;
@@ -254,8 +259,19 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
     __syncthreads();
     const int64_t nmask = a.n - 1;
     const double inv_n = a.pr.fac;
+    // A forward + inverse row starts and ends with the stage-0 positions of
+    // each thread, so the next row may overwrite the data buffer without a
+    // barrier; every other flow ends its row with one.
+    const bool paired = (flags & PF_FWD) && (flags & PF_INV) && !(flags & PF_SPEC_IN);
 
-    for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int fbase = B::freq_base(tp);  // per-thread part of the spectrum indices
+
+    int parity = 0;
+    for (int64_t row = blockIdx.x; row < rows; row += gridDim.x, parity ^= 1) {
+        // per-row tables, double-buffered by row parity: the next row fills
+        // the other copy while slower warps still read this one
+        Cx *vec = tw + B::TW + parity * (NV + 64 + NQ);  // four-step factors: [0,64) low, [64, NV) high
+        Cx *chp = vec + NV;  // chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
         const int64_t k1 = digitrev_rt(row, a.log_n1);
         if (CHIRP && a.pr.has_h) {
             // phase of row k1: G k1^2 + g1 k2s with g1 = 2 N1 G k1 (turns);
@@ -302,23 +318,29 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         }
 
         if constexpr (CHIRP) {
-          if (a.pr.has_h) {
-            // H = P[k2s & 63] * Q[k2s >> 6] * h3[r][tp], zero in the cutoff range
-            const int half2 = 1 << (LOG_L2 - 1);
-            const Cx *h3 = static_cast<const Cx *>(a.pr.h3);
-#pragma unroll
-            for (int r = 0; r < E; ++r) {
-                const int k2 = B::last_freq(tp, r);
-                const int64_t k = k1 + (int64_t(k2) << a.log_n1);
-                const int k2s = k2 >= half2 ? k2 - 2 * half2 : k2;
-                const Cx h = cmul(cmul(chp[k2s & 63], chp[64 + (k2s >> 6) + NQ / 2]), __ldg(h3 + r * B::T + tp));
-                v[r] = (a.pr.has_cut && k >= a.pr.cut_lo && k < a.pr.cut_hi) ? Cx{} : cmul(v[r], h);
+          if (a.pr.has_h || a.pr.has_cut) {
+            // cutoff: k = k1 + k2 N1 in [cut_lo, cut_hi)  <=>  k2 in [k2lo, k2hi)
+            int k2lo = 0, k2hi = 0;
+            if (a.pr.has_cut) {
+                k2lo = k2_bound(a.pr.cut_lo - k1, a.log_n1, L);
+                k2hi = k2_bound(a.pr.cut_hi - k1, a.log_n1, L);
             }
-          } else if (a.pr.has_cut) {
+            const unsigned cut_span = unsigned(k2hi - k2lo);
+            if (a.pr.has_h) {
+                // H = P[k2s & 63] * Q[k2s >> 6] * h3[r][tp]; k2 >= L/2 (k2s = k2 - L)
+                // is decided by the compile-time part of the frequency
+                const Cx *h3 = static_cast<const Cx *>(a.pr.h3);
 #pragma unroll
-            for (int r = 0; r < E; ++r) {
-                const int64_t k = k1 + (int64_t(B::last_freq(tp, r)) << a.log_n1);
-                if (k >= a.pr.cut_lo && k < a.pr.cut_hi) v[r] = Cx{};
+                for (int r = 0; r < E; ++r) {
+                    const int k2 = fbase | B::freq_off(r);
+                    const int k2s = (B::freq_off(r) & (L >> 1)) ? k2 - L : k2;
+                    const Cx h = cmul(cmul(chp[k2s & 63], chp[64 + (k2s >> 6) + NQ / 2]), __ldg(h3 + r * B::T + tp));
+                    v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : cmul(v[r], h);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < E; ++r)
+                    if (unsigned((fbase | B::freq_off(r)) - k2lo) < cut_span) v[r] = Cx{};
             }
           }
         } else if (a.pr.has_h || a.pr.has_cut) {
@@ -352,7 +374,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[B::last_pos(tp, r)] = v[r];
         }
-        __syncthreads();
+        if (!paired) __syncthreads();
     }
 }
 
@@ -369,15 +391,21 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     const int tp = t / C;
     Cx *sm = reinterpret_cast<Cx *>(smraw) + c * B::PITCH;
     Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
-    Cx *vec = tw + B::TW;  // per-column four-step factors, NV per column
     const int log_n2 = a.log_n2;
     const int flags = a.flags;
     const int64_t tiles = (int64_t(1) << log_n2) / C;
     const int64_t nmask = a.n - 1;
     B::load_twiddles(tw, static_cast<const Cx *>(a.tw_col));
     __syncthreads();
+    // An inverse + forward tile starts and ends with the last-stage positions
+    // of each thread, so the next tile may overwrite the data buffer without
+    // a barrier; every other flow ends its tile with one.
+    const bool paired = (flags & PF_FWD) && (flags & PF_INV);
 
-    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    int parity = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, parity ^= 1) {
+        // per-column four-step factors (NV per column), double-buffered by tile parity
+        Cx *vec = tw + B::TW + parity * (C * NVP);
         const int64_t col0 = tile * C;
         const int64_t col = col0 + c;
         if (flags & PF_TW) {
@@ -421,7 +449,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[int64_t(B::first_pos(tp, r)) << log_n2] = v[r];
         }
-        __syncthreads();
+        if (!paired) __syncthreads();
     }
 }
 
@@ -461,7 +489,7 @@ template <int L> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) 
 template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
     auto k = row_pass_kernel<Real, LG, E, CH>;
-    const size_t smem = B::SMEM + size_t(n_vec<B::L>() + n_chirp<B::L>()) * sizeof(typename B::Cx);
+    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L>()) * sizeof(typename B::Cx);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
@@ -474,7 +502,7 @@ template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(con
 template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
     auto k = col_pass_kernel<Real, LG, C, E>;
-    const size_t smem = B::SMEM + size_t(C) * (n_vec<B::L>() | 1) * sizeof(typename B::Cx);
+    const size_t smem = B::SMEM + 2 * size_t(C) * (n_vec<B::L>() | 1) * sizeof(typename B::Cx);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);

@@ -1,0 +1,150 @@
+"""Simulation-directory drop-in: run one source of a rave-sim simulation
+directory on the engine and write its ``detected.npy``.
+
+The directory layout is the reference's (big-wave/Readme.md, written by
+``multisim.setup_simulation``, big-wave/multisim.py:282-521):
+
+    <sim_dir>/config.yaml        sim_params, elements, dtype, save_final_u_vectors, ...
+    <sim_dir>/computed.yaml      cutoff_angles (len(elements)+1), ...
+    <sim_dir>/<grid>.npy         int8 sample grids named by the elements' grid_path
+    <sim_dir>/NNNNNNNN/subconfig.yaml   energy, source, deltabeta_table
+
+``run_single_simulation`` mirrors ``multisim.run_single_simulation``
+(big-wave/multisim.py:50-150): it writes ``NNNNNNNN/detected.npy`` (float64,
+shape (nr_phase_steps, nr_pixels)) and, with ``save_final_u_vectors`` and no
+phase stepping, ``NNNNNNNN/u_0000.npy``. The command line mirrors fast-wave's
+``fastwave <sim_dir> -s <idx>`` (fast-wave/main.cpp:18-57):
+
+    python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16]
+
+The field stays in GPU memory for the whole source, so ``use_disk_vector`` is
+accepted and ignored. History recording (``--history_dz``) and keypoints are
+not supported: they record intermediate fields, which the fused engine never
+forms.
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+import yaml
+
+
+def sub_dir(sim_dir: Path, source_idx: int) -> Path:
+    """``util.get_sub_dir`` (big-wave/util.py:92-97)."""
+    return Path(sim_dir) / f"{source_idx:08}"
+
+
+def _load(path: Path):
+    with open(path) as f:
+        return yaml.safe_load(f)
+
+
+def _dtype(config) -> str:
+    """``config.parse_dtype`` (big-wave/config.py:171-188): default c16."""
+    val = config.get("dtype", "c16")
+    if val not in ("c8", "c16"):
+        raise ValueError(f"Unknown dtype: {val}. Has to be either c8 or c16")
+    return val
+
+
+def load_source(sim_dir, source_idx: int) -> dict:
+    """Everything one source needs, in the case schema used by the engine:
+    the config keys plus ``cutoff_angles``, ``energy``, ``db``, ``source``
+    and the sample grids (``grids``: element index -> int8 array)."""
+    sim_dir = Path(sim_dir)
+    config = _load(sim_dir / "config.yaml")
+    computed = _load(sim_dir / "computed.yaml")
+    sub = _load(sub_dir(sim_dir, source_idx) / "subconfig.yaml")
+    els = []
+    grids = {}
+    for i, el in enumerate(config["elements"]):
+        t = el["type"]
+        if t == "save_and_exit":
+            raise ValueError("save_and_exit elements are resolved by the setup; run the reduced config")
+        if t == "sample":
+            g = np.load(sim_dir / el["grid_path"])
+            if g.dtype != np.int8:
+                raise AssertionError("sample grids must be int8")
+            grids[i] = g
+        if t not in ("grating", "dba_grating", "sample"):
+            raise ValueError(f"Unknown optical element type: {t}.")
+        els.append(dict(el))
+    angles = [float(a) for a in computed["cutoff_angles"]]
+    if len(angles) != len(els) + 1:
+        raise AssertionError("computed.yaml must hold len(elements) + 1 cutoff angles")
+    src = sub["source"]
+    if src["type"] == "point":
+        source = {"type": "point", "x": float(src["x"]), "z": float(src["z"])}
+    elif src["type"] == "vector":
+        source = {"type": "vector", "z": float(src["z"]), "path": str(src["input_path"])}
+    else:
+        raise ValueError(f'Unknown source type: {src["type"]}.')
+    return {
+        "sim_params": dict(config["sim_params"]),
+        "elements": els,
+        "dtype": _dtype(config),
+        "save_final_u_vectors": bool(config.get("save_final_u_vectors", False)),
+        "cutoff_angles": angles,
+        "energy": float(sub["energy"]),
+        "db": [[list(m), list(v)] for m, v in sub["deltabeta_table"]],
+        "source": source,
+        "grids": grids,
+    }
+
+
+def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, dtype: Optional[str] = None,
+                          history_dz: Optional[float] = None) -> np.ndarray:
+    """Run source ``source_idx`` of ``sim_dir`` and write its detected.npy
+    (big-wave/multisim.py:50-150). Returns the detector array."""
+    if history_dz is not None:
+        raise ValueError("history recording is not supported by the fused engine")
+    from .engine import Simulation
+
+    sim_dir = Path(sim_dir)
+    c = load_source(sim_dir, source_idx)
+    dt = dtype or c["dtype"]
+    field = None
+    if c["source"]["type"] == "vector":
+        field = np.load(c["source"]["path"])
+        want = np.complex128 if dt == "c16" else np.complex64
+        if field.dtype != want:
+            field = field.astype(want)  # the reference converts with a warning (config.py:155-160)
+    sim = Simulation(c, grids=c["grids"], dtype=dt, cutoff_angles=c["cutoff_angles"])
+    try:
+        sim.reset()
+        sim.run_source(energy=c["energy"], db_table=c["db"], source=c["source"], field=field)
+        det = sim.detected()
+        out_dir = sub_dir(sim_dir, source_idx)
+        np.save(out_dir / "detected.npy", det)
+        if c["save_final_u_vectors"]:
+            if det.shape[0] != 1:
+                raise ValueError("save_final_u_vectors with phase stepping is not supported")
+            np.save(out_dir / "u_0000.npy", sim.final_field().cpu().numpy())
+        return det
+    finally:
+        sim.close()
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m rave_sim_b200.simdir",
+                                 description="Run one source of a rave-sim simulation directory on the GPU engine.")
+    ap.add_argument("sim_dir")
+    ap.add_argument("-s", "--source_idx", type=int, required=True)
+    ap.add_argument("--dtype", choices=["c8", "c16"], default=None, help="override the config's dtype")
+    ap.add_argument("--history_dz", type=float, default=None)
+    a = ap.parse_args(argv)
+    try:
+        run_single_simulation(a.sim_dir, a.source_idx, dtype=a.dtype, history_dz=a.history_dz)
+    except Exception as e:  # mirror fastwave: message and non-zero exit, no traceback
+        print(f"error: {e}", file=sys.stderr)
+        return 1
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
