@@ -62,9 +62,11 @@ double rsw_energy_to_wavelength(double energy_ev);
 
 /* ------------------------------------------------------------ FFT plans
  * Replaces fast-wave's FFT<S> (fast-wave/src/fft.hpp:9-24, src/fft.cpp:6-48):
- * a 1-D complex FFT of length N (a power of two, 16 <= N <= 2^26 for C64 and
- * 2^24 for C128 in this version), forward unnormalised, inverse scaled by 1/N
- * (the reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length.
+ * a 1-D complex FFT of length N (a power of two, 16 <= N <= 2^38 for C64 and
+ * 2^35 for C128), forward unnormalised, inverse scaled by 1/N (the
+ * reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length. Up to
+ * 2^26 (C64) / 2^24 (C128) a split step costs two passes over the field,
+ * beyond that four (three-level plans). log_rows + log_cols = log2 N.
  * The plan owns its twiddle tables and scratch; it is bound to the device that
  * is current at creation. */
 rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype);
@@ -233,7 +235,8 @@ rsw_status rsw_sim_accumulator(rsw_sim sim, double **d_acc);
 rsw_status rsw_sim_final_field(rsw_sim sim, void *d_dst, void *stream);
 
 /* Per-kernel-kind device timing of the next rsw_sim_run calls (CUDA events on
- * the run's stream). kind: 0 = row pass, 1 = column pass, 2 = detection.
+ * the run's stream). kind: 0 = row pass, 1 = column pass, 2 = detection,
+ * 3 = middle pass (three-level plans, N above the two-level limit).
  * rsw_sim_timing returns the summed milliseconds and launch counts since
  * enabling; it synchronises. */
 rsw_status rsw_sim_set_timing(rsw_sim sim, int enable);

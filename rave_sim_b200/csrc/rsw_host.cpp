@@ -28,10 +28,10 @@
 namespace rsw {
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
-cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
-                                   cudaStream_t s);
-cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
-                                   cudaStream_t s);
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
+                                   bool dbl, cudaStream_t s);
+cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
+                                   bool dbl, cudaStream_t s);
 cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cudaStream_t s);
 cudaError_t launch_copy(const void *in, void *out, int64_t n, bool dbl, cudaStream_t s);
 cudaError_t launch_point_source(void *u, int64_t n, double dx, double w, double z, double x_src, bool dbl,
@@ -292,11 +292,12 @@ struct rsw_plan_s {
     int64_t n = 0;
     int log_n = 0;
     int dtype = RSW_C128;
-    int log_n1 = 0, log_n2 = 0;  // column level, row level
+    int log_n1 = 0, log_n2 = 0;  // column level, row level: N = N1 * N2
+    int log_nb = 0, log_nr = 0;  // N2 = Nb * Nr: middle level (0: two-level) and row-kernel length
     int device = 0;
-    int row_e = 16, col_e = 16;  // elements per thread of the row / column kernels
-    DevBuf tw_row, tw_col, tw4_lo, tw4_hi;
-    int tw4_shift = 0;
+    int row_e = 16, col_e = 16, mid_e = 16;  // elements per thread of the row / column / middle kernels
+    DevBuf tw_row, tw_col, tw_mid, tw4_lo, tw4_hi, tw4b_lo, tw4b_hi;
+    int tw4_shift = 0, tw4b_shift = 0;
     DevBuf scratch;                                       // N samples, for the natural-order APIs
     DevBuf det_bounds, det_cos, det_r;                    // cached detector geometry
     double det_key[5] = {0, 0, 0, 0, 0};
@@ -306,6 +307,7 @@ struct rsw_plan_s {
     DevBuf h3_call;                                       // per-call chirp table
     bool dbl() const { return dtype == RSW_C128; }
     size_t elem() const { return dbl() ? 16 : 8; }
+    bool three() const { return log_nb > 0; }
 };
 
 // W_M^m = exp(-2 pi i m / M), accurate to < 1 ulp (long double evaluation)
@@ -339,65 +341,106 @@ template <typename T> static std::vector<T> block_twiddles(int log_l) {
     return v;
 }
 
+// four-step twiddles W_M^m = lo[m & (2^h - 1)] * hi[m >> h] of M = 2^log_m in
+// FP64 for both dtypes (rounded per tile on the device)
+static rsw_status four_step_tables(int log_m, DevBuf &lo_buf, DevBuf &hi_buf, int *shift) {
+    const int h = (log_m + 1) / 2;
+    const int64_t m = int64_t(1) << log_m;
+    *shift = h;
+    std::vector<double> lo, hi;
+    for (int64_t a = 0; a < (int64_t(1) << h); ++a) push_c(lo, twiddle(a, m));
+    for (int64_t b = 0; b < (int64_t(1) << (log_m - h)); ++b) push_c(hi, twiddle(b << h, m));
+    CHECK(lo_buf.upload(lo));
+    return hi_buf.upload(hi);
+}
+
 template <typename T> static rsw_status plan_tables(rsw_plan_s *p) {
-    CHECK(p->tw_row.upload(block_twiddles<T>(p->log_n2)));
+    CHECK(p->tw_row.upload(block_twiddles<T>(p->log_nr)));
     if (p->log_n1 > 0) {
         CHECK(p->tw_col.upload(block_twiddles<T>(p->log_n1)));
-        // four-step twiddles in FP64 for both dtypes (rounded per tile on the device)
-        const int h = (p->log_n + 1) / 2;
-        p->tw4_shift = h;
-        std::vector<double> lo, hi;
-        for (int64_t a = 0; a < (int64_t(1) << h); ++a) push_c(lo, twiddle(a, p->n));
-        for (int64_t b = 0; b < (int64_t(1) << (p->log_n - h)); ++b) push_c(hi, twiddle(b << h, p->n));
-        CHECK(p->tw4_lo.upload(lo));
-        CHECK(p->tw4_hi.upload(hi));
+        CHECK(four_step_tables(p->log_n, p->tw4_lo, p->tw4_hi, &p->tw4_shift));
+    }
+    if (p->three()) {
+        CHECK(p->tw_mid.upload(block_twiddles<T>(p->log_nb)));
+        CHECK(four_step_tables(p->log_n2, p->tw4b_lo, p->tw4b_hi, &p->tw4b_shift));
     }
     return RSW_OK;
 }
 
-static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *l2) {
+// Level split of N = 2^lg: one row level up to the row kernel's limit; two
+// levels (columns x rows) up to the column limit times the row limit; beyond
+// that three levels, N = N1 x Nb x Nr, with rows of the row kernel's maximum
+// length and the rest split evenly between the outer column level and the
+// middle level (both run by the column kernel).
+static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb, int *lr) {
     if (n < 16 || (n & (n - 1)) != 0)
         return fail(RSW_ERR_UNSUPPORTED, "N = %lld: this version supports powers of two >= 16", (long long)n);
     int lg = 0;
     while ((int64_t(1) << lg) < n) ++lg;
     const int row_max = dtype == RSW_C128 ? ROW_MAX_C128 : ROW_MAX_C64;
     const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
+    *log_n = lg;
+    *lb = 0;
+    // RSW_SPLIT3 = "l1,lb,lr" forces a three-level split (tests and tuning sweeps)
+    const char *ov3 = std::getenv("RSW_SPLIT3");
+    if (ov3 && *ov3) {
+        int a = 0, b = 0, c = 0;
+        if (std::sscanf(ov3, "%d,%d,%d", &a, &b, &c) == 3 && a + b + c == lg && a >= 4 && a <= col_max &&
+            b >= 4 && b <= col_max && c >= 7 && c <= row_max) {
+            *l1 = a;
+            *lb = b;
+            *lr = c;
+            return RSW_OK;
+        }
+    }
     if (lg <= row_max) {
         *l1 = 0;
-        *l2 = lg;
-    } else {
-        // prefer columns of at most 2^11 (the 2^12 c64 column kernel runs 1024
-        // threads at 64 registers and spills); rows take the rest
-        int a = std::min(std::min(col_max, 11), lg / 2);
-        int b = lg - a;
-        if (b > row_max) {
-            a = lg - row_max;
-            b = row_max;
-        }
-        if (b < 7) {  // rows of two-level plans hold at least 2^7 samples
-            b = 7;
-            a = lg - b;
-        }
-        if (b > row_max) {
-            a = lg - row_max;
-            b = row_max;
-        }
-        if (a > col_max || a < 4)
-            return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the two-level limit 2^%d for this dtype", lg,
-                        row_max + col_max);
-        // RSW_SPLIT overrides the column level (tuning sweeps) when valid
-        const char *ov = std::getenv("RSW_SPLIT");
-        if (ov && *ov) {
-            const int oa = std::atoi(ov), ob = lg - oa;
-            if (oa >= 4 && oa <= col_max && ob >= 7 && ob <= row_max) {
-                a = oa;
-                b = ob;
-            }
-        }
-        *l1 = a;
-        *l2 = b;
+        *lr = lg;
+        return RSW_OK;
     }
-    *log_n = lg;
+    if (lg > row_max + col_max) {
+        if (lg > row_max + 2 * col_max)
+            return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the three-level limit 2^%d for this dtype", lg,
+                        row_max + 2 * col_max);
+        // outer columns of at least 2^7 (the pass with the transmission and
+        // the twiddle tables); the middle level runs plain FFTs
+        const int rest = lg - row_max;
+        *lr = row_max;
+        *l1 = std::max(7, (rest + 1) / 2);
+        *lb = rest - *l1;
+        if (*lb < 4) {
+            *lb = 4;
+            *l1 = rest - 4;
+        }
+        return RSW_OK;
+    }
+    // prefer columns of at most 2^11 (the 2^12 c64 column kernel runs 1024
+    // threads at 64 registers and spills); rows take the rest
+    int a = std::min(std::min(col_max, 11), lg / 2);
+    int b = lg - a;
+    if (b > row_max) {
+        a = lg - row_max;
+        b = row_max;
+    }
+    if (b < 7) {  // rows of two-level plans hold at least 2^7 samples
+        b = 7;
+        a = lg - b;
+    }
+    if (b > row_max) {
+        a = lg - row_max;
+        b = row_max;
+    }
+    // RSW_SPLIT overrides the column level (tuning sweeps) when valid
+    const char *ov = std::getenv("RSW_SPLIT");
+    if (ov && *ov) {
+        const int oa = std::atoi(ov), ob = lg - oa;
+        if (oa >= 4 && oa <= col_max && ob >= 7 && ob <= row_max) {
+            a = oa;
+            b = ob;
+        }
+    }
+    *l1 = a;
+    *lr = b;
     return RSW_OK;
 }
 
@@ -410,13 +453,24 @@ static int env_int(const char *name, int dflt) {
 }
 static void choose_tuning(rsw_plan_s *p) {
     auto pick = [](int log_l, int dflt) { return log_l >= 9 ? dflt : 16; };
-    p->row_e = pick(p->log_n2, 16);
+    p->row_e = pick(p->log_nr, 16);
     p->col_e = pick(p->log_n1, 16);
+    p->mid_e = pick(p->log_nb, 16);
     const int re = env_int("RSW_ROW_E", 0), ce = env_int("RSW_COL_E", 0);
-    if ((re == 16 || re == 32) && p->log_n2 >= 9) p->row_e = re;
+    if ((re == 16 || re == 32) && p->log_nr >= 9) p->row_e = re;
     if ((ce == 16 || ce == 32) && p->log_n1 >= 9) p->col_e = ce;
 }
 
+// Arguments of the outer column pass (and of single-level row passes).
+//
+// Between split steps the field is kept in the "mid" layout: the column
+// spectrum (row p1 holds column frequency k1 = digitrev(p1)) with the row
+// level already inverted. The column pass applies W_N^(n2 k1) after its
+// forward (PF_TW). Two-level plans apply conj(W_N^(n2 k1)) / N at the end of
+// the row pass (PF_TW of the row kernel). Three-level plans apply it in the
+// column pass before the inverse (PF_TWI, from the same factor table) and
+// W_{N2}^(nr kb) around the row transform (PF_TWF before, PF_TW after), so
+// that their middle passes are plain FFTs.
 static PassArgs base_args(const rsw_plan_s *p) {
     PassArgs a{};
     a.n = p->n;
@@ -427,7 +481,39 @@ static PassArgs base_args(const rsw_plan_s *p) {
     a.tw4_lo = p->tw4_lo.p;
     a.tw4_hi = p->tw4_hi.p;
     a.tw4_shift = p->tw4_shift;
+    a.tw_log = p->log_n;
+    a.tw_scale = 1.0 / double(p->n);
     a.pr.fac = 1.0 / double(p->n);
+    a.tr.kind = TR_NONE;
+    return a;
+}
+// The same arguments for the row kernel: rows of Nr samples; in three-level
+// plans its twiddles are W_{N2}^(nr kb), unscaled.
+static PassArgs row_level(const rsw_plan_s *p, PassArgs a) {
+    a.log_n2 = p->log_nr;
+    a.log_nb = p->log_nb;
+    if (p->three()) {
+        a.tw4_lo = p->tw4b_lo.p;
+        a.tw4_hi = p->tw4b_hi.p;
+        a.tw4_shift = p->tw4b_shift;
+        a.tw_log = p->log_n2;
+        a.tw_scale = 1.0;
+    }
+    return a;
+}
+// row-pass twiddle flags of a multi-level plan
+static int row_tw(const rsw_plan_s *p, bool fwd, bool inv) {
+    return p->three() ? ((fwd ? PF_TWF : 0) | (inv ? PF_TW : 0)) : (inv ? PF_TW : 0);
+}
+// column-pass flags of the inverse of the "mid" layout
+static int col_inv(const rsw_plan_s *p) { return PF_INV | (p->three() ? PF_TWI : 0); }
+// The middle level of three-level plans: the column kernel over N1 batches
+// of Nb x Nr, a plain FFT over nb.
+static PassArgs mid_level(const rsw_plan_s *p, PassArgs a) {
+    a.log_n1 = p->log_nb;
+    a.log_n2 = p->log_nr;
+    a.log_nb = 0;
+    a.tw_col = p->tw_mid.p;
     a.tr.kind = TR_NONE;
     return a;
 }
@@ -441,8 +527,8 @@ struct TimingLog {
     };
     std::vector<Rec> recs;
     std::vector<cudaEvent_t> pool;
-    double ms[3] = {0, 0, 0};
-    int64_t launches[3] = {0, 0, 0};
+    double ms[4] = {0, 0, 0, 0};  // row, column, detect, middle
+    int64_t launches[4] = {0, 0, 0, 0};
     cudaEvent_t get() {
         if (!pool.empty()) {
             cudaEvent_t e = pool.back();
@@ -500,15 +586,28 @@ static rsw_status run_col(const rsw_plan_s *p, const PassArgs &a, cudaStream_t s
     if (tl && tl->enabled) tl->end(r, s);
     return RSW_OK;
 }
+// middle pass of a three-level plan
+static rsw_status run_mid(const rsw_plan_s *p, const PassArgs &base, bool forward, cudaStream_t s,
+                          TimingLog *tl = nullptr) {
+    PassArgs a = mid_level(p, base);
+    a.flags = forward ? PF_FWD : PF_INV;
+    TimingLog::Rec r{};
+    if (tl && tl->enabled) tl->begin(3, s, r);
+    cudaError_t e = launch_col_pass(a, p->dbl(), p->mid_e, s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "middle pass (2^%d): %s", a.log_n1, cudaGetErrorString(e));
+    if (tl && tl->enabled) tl->end(r, s);
+    return RSW_OK;
+}
 
-// Build the row-level chirp table of a transfer function into `table` (N2
-// samples) and switch `pr` to the chirp form. Two-level plans only.
+// Build the row-level chirp table of a transfer function into `table` (Nr
+// samples) and switch `pr` to the chirp form. Multi-level plans only: the
+// spectrum index of a row sample is kbase + M k2 with M = N1 Nb.
 static rsw_status prepare_chirp(const rsw_plan_s *p, PropArgs &pr, void *table, cudaStream_t s) {
     if (p->log_n1 == 0 || !pr.has_h) return RSW_OK;
     double g_hi, g_lo;
     chirp_constant(pr, p->n, &g_hi, &g_lo);
-    const double n1sq = std::ldexp(1.0, 2 * p->log_n1);  // exact power of two
-    cudaError_t e = launch_chirp_table(table, p->log_n2, g_hi * n1sq, g_lo * n1sq, p->dbl(), p->row_e, s);
+    const double msq = std::ldexp(1.0, 2 * (p->log_n1 + p->log_nb));  // exact power of two
+    cudaError_t e = launch_chirp_table(table, p->log_nr, g_hi * msq, g_lo * msq, p->dbl(), p->row_e, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "chirp table: %s", cudaGetErrorString(e));
     pr.chirp = 1;
     pr.g_hi = g_hi;
@@ -538,15 +637,17 @@ rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
     if (!out) return fail(RSW_ERR_INVALID, "out is NULL");
     *out = nullptr;
     if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
-    int lg, l1, l2;
-    CHECK(plan_split(n, dtype, &lg, &l1, &l2));
+    int lg, l1, lb, lr;
+    CHECK(plan_split(n, dtype, &lg, &l1, &lb, &lr));
     std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
     if (!p) return fail(RSW_ERR_NOMEM, "host allocation failed");
     p->n = n;
     p->log_n = lg;
     p->dtype = dtype;
     p->log_n1 = l1;
-    p->log_n2 = l2;
+    p->log_nb = lb;
+    p->log_nr = lr;
+    p->log_n2 = lb + lr;
     CU(cudaGetDevice(&p->device));
     choose_tuning(p.get());
     CHECK(p->dbl() ? plan_tables<double>(p.get()) : plan_tables<float>(p.get()));
@@ -571,25 +672,30 @@ rsw_status rsw_plan_info(rsw_plan p, int64_t *n, int *dtype, int *log_rows, int 
 
 static rsw_status need_scratch(rsw_plan_s *p) { return p->scratch.alloc(size_t(p->n) * p->elem()); }
 
+static cudaError_t to_natural(const rsw_plan_s *p, const void *spec, void *nat, cudaStream_t s) {
+    return launch_spec_to_natural(spec, nat, p->n, p->log_n1, p->log_nb, p->log_nr, p->dbl(), s);
+}
+static cudaError_t to_spec(const rsw_plan_s *p, const void *nat, void *spec, cudaStream_t s) {
+    return launch_natural_to_spec(nat, spec, p->n, p->log_n1, p->log_nb, p->log_nr, p->dbl(), s);
+}
+
 rsw_status rsw_fft_forward(rsw_plan p, const void *in, void *out, void *stream) {
     if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
     cudaStream_t s = (cudaStream_t)stream;
     CHECK(need_scratch(p));
     PassArgs a = base_args(p);
+    a.in = in;
+    a.out = p->scratch.p;
     if (p->log_n1 > 0) {
-        a.in = in;
-        a.out = p->scratch.p;
         a.flags = PF_FWD | PF_TW;
         CHECK(run_col(p, a, s));
         a.in = p->scratch.p;
-    } else {
-        a.in = in;
-        a.out = p->scratch.p;
+        if (p->three()) CHECK(run_mid(p, a, true, s));
     }
-    a.out = p->scratch.p;
-    a.flags = PF_FWD;
-    CHECK(run_row(p, a, s));
-    cudaError_t e = launch_spec_to_natural(p->scratch.p, out, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+    PassArgs r = row_level(p, a);
+    r.flags = PF_FWD | row_tw(p, true, false);
+    CHECK(run_row(p, r, s));
+    cudaError_t e = to_natural(p, p->scratch.p, out, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
     return RSW_OK;
 }
@@ -598,17 +704,19 @@ rsw_status rsw_fft_inverse(rsw_plan p, const void *in, void *out, void *stream) 
     if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
     cudaStream_t s = (cudaStream_t)stream;
     CHECK(need_scratch(p));
-    cudaError_t e = launch_natural_to_spec(in, p->scratch.p, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+    cudaError_t e = to_spec(p, in, p->scratch.p, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
     PassArgs a = base_args(p);
     a.in = p->scratch.p;
     if (p->log_n1 > 0) {
+        PassArgs r = row_level(p, a);
+        r.out = p->scratch.p;
+        r.flags = PF_SPEC_IN | PF_INV | row_tw(p, false, true);
+        CHECK(run_row(p, r, s));
         a.out = p->scratch.p;
-        a.flags = PF_SPEC_IN | PF_INV | PF_TW;
-        CHECK(run_row(p, a, s));
-        a.in = p->scratch.p;
+        if (p->three()) CHECK(run_mid(p, a, false, s));
         a.out = out;
-        a.flags = PF_INV;
+        a.flags = col_inv(p);
         CHECK(run_col(p, a, s));
     } else {
         a.out = out;
@@ -628,38 +736,42 @@ rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, dou
     a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0);
     const bool two = p->log_n1 > 0;
     if (two && a.pr.has_h) {
-        CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_n2) * p->elem()));
+        CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_nr) * p->elem()));
         CHECK(prepare_chirp(p, a.pr, p->h3_call.p, s));
-    }
-    // 1. spectrum of u in the internal layout, in place in u
-    if (skip_fft) {
-        cudaError_t e = launch_natural_to_spec(U, u, p->n, p->log_n1, p->log_n2, p->dbl(), s);
-        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
-    } else if (two) {
-        a.in = u;
-        a.out = u;
-        a.flags = PF_FWD | PF_TW;
-        CHECK(run_col(p, a, s));
     }
     a.in = u;
     a.out = u;
+    // 1. spectrum of u in the internal layout, in place in u
+    if (skip_fft) {
+        cudaError_t e = to_spec(p, U, u, s);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+    } else if (two) {
+        PassArgs c = a;
+        c.pr = PropArgs{};
+        c.flags = PF_FWD | PF_TW;
+        CHECK(run_col(p, c, s));
+        if (p->three()) CHECK(run_mid(p, c, true, s));
+    }
+    PassArgs r = two ? row_level(p, a) : a;
     if (U) {
         // 2a. forward row level + transfer function, spectrum out; copy to U in natural order
-        a.flags = skip_fft ? PF_SPEC_IN : PF_FWD;
-        CHECK(run_row(p, a, s));
-        cudaError_t e = launch_spec_to_natural(u, U, p->n, p->log_n1, p->log_n2, p->dbl(), s);
+        r.flags = skip_fft ? PF_SPEC_IN : (PF_FWD | row_tw(p, true, false));
+        CHECK(run_row(p, r, s));
+        cudaError_t e = to_natural(p, u, U, s);
         if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
-        a.pr.has_h = 0;
-        a.pr.has_cut = 0;
-        a.flags = PF_SPEC_IN | PF_INV | (two ? PF_TW : PF_SCALE);
-        CHECK(run_row(p, a, s));
+        r.pr.has_h = 0;
+        r.pr.has_cut = 0;
+        r.flags = PF_SPEC_IN | PF_INV | (two ? row_tw(p, false, true) : PF_SCALE);
+        CHECK(run_row(p, r, s));
     } else {
-        a.flags = (skip_fft ? PF_SPEC_IN : PF_FWD) | PF_INV | (two ? PF_TW : PF_SCALE);
-        CHECK(run_row(p, a, s));
+        r.flags = (skip_fft ? PF_SPEC_IN : (PF_FWD | row_tw(p, true, false))) | PF_INV |
+                  (two ? row_tw(p, false, true) : PF_SCALE);
+        CHECK(run_row(p, r, s));
     }
     if (two) {
         a.pr = PropArgs{};
-        a.flags = PF_INV;
+        if (p->three()) CHECK(run_mid(p, a, false, s));
+        a.flags = col_inv(p);
         CHECK(run_col(p, a, s));
     }
     return RSW_OK;
@@ -911,7 +1023,7 @@ struct Runner {
         if (fresh) {
             chirp_dz.push_back(dz);
             if (S->h3_pool.size() <= slot) S->h3_pool.emplace_back(new DevBuf());
-            CHECK(S->h3_pool[slot]->alloc(size_t(int64_t(1) << P->log_n2) * P->elem()));
+            CHECK(S->h3_pool[slot]->alloc(size_t(int64_t(1) << P->log_nr) * P->elem()));
             CHECK(prepare_chirp(P, pr, S->h3_pool[slot]->p, st));
             return RSW_OK;
         }
@@ -938,15 +1050,22 @@ struct Runner {
         if (P->log_n1 > 0) {
             a.in = ones ? nullptr : S->buf[cur].p;
             a.out = S->buf[dst].p;
-            a.flags = (mid ? PF_INV : 0) | PF_FWD | PF_TW | (tr.kind != TR_NONE ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
+            a.flags = (mid ? col_inv(P) : 0) | PF_FWD | PF_TW | (tr.kind != TR_NONE ? PF_TRANS : 0) |
+                      (ones ? PF_ONES : 0);
             PropArgs keep = a.pr;
             a.pr = PropArgs{};
             CHECK(run_col(P, a, st, &S->tl));
-            a.pr = keep;
             a.in = S->buf[dst].p;
             a.tr.kind = TR_NONE;
-            a.flags = PF_FWD | PF_INV | PF_TW;
-            CHECK(run_row(P, a, st, &S->tl));
+            if (P->three()) CHECK(run_mid(P, a, true, st, &S->tl));
+            a.pr = keep;
+            PassArgs r = row_level(P, a);
+            r.flags = PF_FWD | PF_INV | row_tw(P, true, true);
+            CHECK(run_row(P, r, st, &S->tl));
+            if (P->three()) {
+                a.pr = PropArgs{};
+                CHECK(run_mid(P, a, false, st, &S->tl));
+            }
             mid = true;
         } else {
             a.in = ones ? nullptr : S->buf[cur].p;
@@ -975,7 +1094,7 @@ struct Runner {
             PassArgs a = base_args(P);
             a.in = S->buf[cur].p;
             a.out = S->buf[dst].p;
-            a.flags = PF_INV;
+            a.flags = col_inv(P);
             CHECK(run_col(P, a, st, &S->tl));
             cur = dst;
             mid = false;
@@ -1207,7 +1326,7 @@ rsw_status rsw_sim_set_timing(rsw_sim S, int enable) {
     if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
     S->tl.collect();
     S->tl.enabled = enable != 0;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < 4; ++k) {
         S->tl.ms[k] = 0;
         S->tl.launches[k] = 0;
     }
@@ -1215,7 +1334,7 @@ rsw_status rsw_sim_set_timing(rsw_sim S, int enable) {
 }
 
 rsw_status rsw_sim_timing(rsw_sim S, int kind, double *ms, int64_t *launches) {
-    if (!S || kind < 0 || kind > 2) return fail(RSW_ERR_INVALID, "bad argument");
+    if (!S || kind < 0 || kind > 3) return fail(RSW_ERR_INVALID, "bad argument");
     S->tl.collect();
     if (ms) *ms = S->tl.ms[kind];
     if (launches) *launches = S->tl.launches[kind];

@@ -60,25 +60,38 @@ struct PropArgs {
 enum PassFlags : int {
     PF_FWD = 1,       // run the forward transform of this level
     PF_INV = 2,       // run the inverse transform of this level
-    PF_TW = 4,        // apply the four-step twiddle (column: after fwd; row: after inv, with 1/N)
+    PF_TW = 4,        // four-step twiddle: column, after fwd: W_M^(n2 k1); row, after inv:
+                      // conj(W_M^(n2 tw_k)) (hi factors times tw_scale)
     PF_TRANS = 8,     // apply transmission (column: between inv and fwd; single-level row: before fwd)
     PF_SCALE = 16,    // single-level row: multiply by 1/N after the inverse
     PF_ONES = 32,     // input is the plane wave u = 1 (input buffer not read)
     PF_SPEC_IN = 64,  // row: input is a spectrum (digit-reversed layout), start with the inverse
+    PF_TWI = 128,     // column: before the inverse, conj(W_M^(n2 k1)) * tw_scale
+    PF_TWF = 256,     // row: before the forward, W_M^(n2 tw_k) (the conjugate of PF_TW's factor)
 };
 
+// Arguments of one pass. N = N1 * N2 samples; three-level plans split the
+// row level further, N2 = Nb * Nr, with a middle pass of the column kernel.
+//   row kernel:    rows of 2^log_n2 samples; row index = p1 * Nb + pb, spectrum
+//                  index k = k1 + N1 * (kb + Nb * k2) with k1 = digitrev(p1),
+//                  kb = digitrev(pb); log_nb = 0 for two-level plans
+//   column kernel: columns of 2^log_n1 samples at stride 2^log_n2, in
+//                  n >> (log_n1 + log_n2) consecutive batches
 struct PassArgs {
     const void *in;
     void *out;
     int64_t n;
-    int log_n1;  // column level (0: single level)
-    int log_n2;  // row level
+    int log_n1;
+    int log_n2;
+    int log_nb;     // row kernel: middle level (0: none)
     int flags;
     const void *tw_row;   // block twiddles of the row level
     const void *tw_col;   // block twiddles of the column level
-    const void *tw4_lo;   // four-step twiddles (FP64): W_N^m = lo[m & mask] * hi[m >> shift]
+    const void *tw4_lo;   // four-step twiddles (FP64): W_M^m = lo[m & mask] * hi[m >> shift], M = 2^tw_log
     const void *tw4_hi;
     int tw4_shift;
+    int tw_log;
+    double tw_scale;      // factor of the conjugate twiddles (1/N at the last inverse level)
     TransArgs tr;
     PropArgs pr;
 };

@@ -36,8 +36,8 @@ namespace rsw {
 rsw_status set_error(rsw_status st, const char *msg);  // message for rsw_last_error()
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
-cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_n2, bool dbl,
-                                   cudaStream_t s);
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
+                                   bool dbl, cudaStream_t s);
 }  // namespace rsw
 
 using namespace rsw;
@@ -166,6 +166,8 @@ extern "C" rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int
     a.tw4_lo = scratch + OFF_TW4LO;
     a.tw4_hi = scratch + OFF_TW4HI;
     a.tw4_shift = (log_n + 1) / 2;
+    a.tw_log = log_n;
+    a.tw_scale = 1.0 / double(n);
     a.pr.fac = 1.0 / double(n);
     void *spec = scratch;
     cudaError_t e;
@@ -181,7 +183,7 @@ extern "C" rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int
     a.out = spec;
     a.flags = PF_FWD;
     if ((e = launch_row_pass(a, dbl, 16, s)) != cudaSuccess) return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
-    if ((e = launch_spec_to_natural(spec, d_out, n, log_n1, log_n2, dbl, s)) != cudaSuccess)
+    if ((e = launch_spec_to_natural(spec, d_out, n, log_n1, 0, log_n2, dbl, s)) != cudaSuccess)
         return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
     return RSW_OK;
 }

@@ -257,8 +257,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
     const int64_t rows = a.n >> LOG_L2;
     B::load_twiddles(tw, static_cast<const Cx *>(a.tw_row));
     __syncthreads();
-    const int64_t nmask = a.n - 1;
-    const double inv_n = a.pr.fac;
+    const int64_t nmask = (int64_t(1) << a.tw_log) - 1;
+    const double tw_scale = a.tw_scale;
+    const int log_m = a.log_n1 + a.log_nb;  // spectrum index k = kbase + 2^log_m * k2
     // A forward + inverse row starts and ends with the stage-0 positions of
     // each thread, so the next row may overwrite the data buffer without a
     // barrier; every other flow ends its row with one.
@@ -272,31 +273,36 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         // the other copy while slower warps still read this one
         Cx *vec = tw + B::TW + parity * (NV + 64 + NQ);  // four-step factors: [0,64) low, [64, NV) high
         Cx *chp = vec + NV;  // chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
-        const int64_t k1 = digitrev_rt(row, a.log_n1);
+        // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
+        // conjugate four-step twiddle of the innermost split uses tw_k
+        const int64_t k1 = digitrev_rt(row >> a.log_nb, a.log_n1);
+        const int64_t kb = digitrev_rt(row & ((int64_t(1) << a.log_nb) - 1), a.log_nb);
+        const int64_t kbase = k1 + (kb << a.log_n1);
+        const int64_t tw_k = a.log_nb > 0 ? kb : k1;
         if (CHIRP && a.pr.has_h) {
-            // phase of row k1: G k1^2 + g1 k2s with g1 = 2 N1 G k1 (turns);
-            // P[a] = A exp(2 pi i (G k1^2 + g1 a)), Q[b] = exp(2 pi i 64 g1 b)
-            const double n1 = double(int64_t(1) << a.log_n1);
-            const double gk = frac_dd(a.pr.g_hi, a.pr.g_lo, double(k1 * k1));
-            const double g1h = 2.0 * n1 * a.pr.g_hi, g1l = 2.0 * n1 * a.pr.g_lo;
+            // phase of the row: G kbase^2 + g1 k2s with g1 = 2 M G kbase (turns),
+            // M = 2^log_m; P[a] = A exp(2 pi i (G kbase^2 + g1 a)), Q[b] = exp(2 pi i 64 g1 b)
+            const double m = double(int64_t(1) << log_m);
+            const double gk = frac_dd(a.pr.g_hi, a.pr.g_lo, double(kbase * kbase));
+            const double g1h = 2.0 * m * a.pr.g_hi, g1l = 2.0 * m * a.pr.g_lo;
             for (int idx = tp; idx < 64 + NQ; idx += B::NT) {
                 double2 w;
                 if (idx < 64) {
-                    w = cmul(a.pr.A, cis_turns(gk + frac_dd(g1h, g1l, double(k1 * idx))));
+                    w = cmul(a.pr.A, cis_turns(gk + frac_dd(g1h, g1l, double(kbase * idx))));
                 } else {
                     const int64_t b = int64_t(idx - 64) - NQ / 2;
-                    w = cis_turns(frac_dd(g1h, g1l, double(k1 * 64 * b)));
+                    w = cis_turns(frac_dd(g1h, g1l, double(kbase * 64 * b)));
                 }
                 chp[idx] = cvt(w, Cx{});
             }
         }
-        if (flags & PF_TW) {
-            // conj(W_N^{n2 k1}) / N = conj(A[n2 & 63]) * conj(B[n2 >> 6]) / N
+        if (flags & (PF_TW | PF_TWF)) {
+            // conj(W_M^{n2 tw_k}) * tw_scale = conj(A[n2 & 63]) * conj(B[n2 >> 6]) * tw_scale
             for (int idx = tp; idx < NV; idx += B::NT) {
-                const int64_t m = ((idx < 64 ? int64_t(idx) : int64_t(idx - 64) << 6) * k1) & nmask;
+                const int64_t m = ((idx < 64 ? int64_t(idx) : int64_t(idx - 64) << 6) * tw_k) & nmask;
                 double2 w = w4(a, m);
                 w = make_double2(w.x, -w.y);
-                if (idx >= 64) w = make_double2(w.x * inv_n, w.y * inv_n);
+                if (idx >= 64) w = make_double2(w.x * tw_scale, w.y * tw_scale);
                 vec[idx] = cvt(w, Cx{});
             }
         }
@@ -307,6 +313,14 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         if (!(flags & PF_SPEC_IN)) {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[B::first_pos(tp, r)];
+            if (flags & PF_TWF) {
+                __syncthreads();  // this row's factor table is complete
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int n2 = B::first_pos(tp, r);
+                    v[r] = cmulc(cmulc(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                }
+            }
             if (flags & PF_TRANS) {
 #pragma unroll
                 for (int r = 0; r < E; ++r) v[r] = apply_trans(a.tr, (row << LOG_L2) + B::first_pos(tp, r), v[r]);
@@ -319,11 +333,11 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
 
         if constexpr (CHIRP) {
           if (a.pr.has_h || a.pr.has_cut) {
-            // cutoff: k = k1 + k2 N1 in [cut_lo, cut_hi)  <=>  k2 in [k2lo, k2hi)
+            // cutoff: k = kbase + k2 2^log_m in [cut_lo, cut_hi)  <=>  k2 in [k2lo, k2hi)
             int k2lo = 0, k2hi = 0;
             if (a.pr.has_cut) {
-                k2lo = k2_bound(a.pr.cut_lo - k1, a.log_n1, L);
-                k2hi = k2_bound(a.pr.cut_hi - k1, a.log_n1, L);
+                k2lo = k2_bound(a.pr.cut_lo - kbase, log_m, L);
+                k2hi = k2_bound(a.pr.cut_hi - kbase, log_m, L);
             }
             const unsigned cut_span = unsigned(k2hi - k2lo);
             if (a.pr.has_h) {
@@ -348,9 +362,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r) {
                 const int64_t k2 = B::last_freq(tp, r);
-                const int64_t k = k1 + (k2 << a.log_n1);
+                const int64_t k = kbase + (k2 << log_m);
                 const int64_t k2s = k2 >= half2 ? k2 - 2 * half2 : k2;
-                const int64_t ks = k1 + k2s * (int64_t(1) << a.log_n1);
+                const int64_t ks = kbase + k2s * (int64_t(1) << log_m);
                 v[r] = prop_apply(a.pr, k, ks, v[r]);
             }
         }
@@ -393,8 +407,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
     const int log_n2 = a.log_n2;
     const int flags = a.flags;
-    const int64_t tiles = (int64_t(1) << log_n2) / C;
-    const int64_t nmask = a.n - 1;
+    const int log_tb = log_n2 - ilog2(C);  // tiles per batch: 2^log_tb
+    const int64_t tiles = (a.n >> LOG_L1) / C;
+    const int64_t nmask = (int64_t(1) << a.tw_log) - 1;
     B::load_twiddles(tw, static_cast<const Cx *>(a.tw_col));
     __syncthreads();
     // An inverse + forward tile starts and ends with the last-stage positions
@@ -406,22 +421,35 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, parity ^= 1) {
         // per-column four-step factors (NV per column), double-buffered by tile parity
         Cx *vec = tw + B::TW + parity * (C * NVP);
-        const int64_t col0 = tile * C;
+        const int64_t batch = tile >> log_tb;
+        const int64_t col0 = (tile & ((int64_t(1) << log_tb) - 1)) * C;  // column within the batch
         const int64_t col = col0 + c;
-        if (flags & PF_TW) {
-            // W_N^{n2 k1} = A[k1 & 63] * B[k1 >> 6] for each of the C columns
+        const int64_t base = batch << (LOG_L1 + log_n2);
+        if (flags & (PF_TW | PF_TWI)) {
+            // W_M^{n2 k1} = A[k1 & 63] * B[k1 >> 6] for each of the C columns
             for (int idx = t; idx < C * NV; idx += B::NT) {
                 const int cc = idx / NV, e = idx % NV;
                 const int64_t m = ((e < 64 ? int64_t(e) : int64_t(e - 64) << 6) * (col0 + cc)) & nmask;
                 vec[cc * NVP + e] = cvt(w4(a, m), Cx{});
             }
         }
-        const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + col;
-        Cx *__restrict__ gout = static_cast<Cx *>(a.out) + col;
+        if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
+        const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + base + col;
+        Cx *__restrict__ gout = static_cast<Cx *>(a.out) + base + col;
         Cx v[E];
         if (flags & PF_INV) {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
+            if (flags & PF_TWI) {
+                __syncthreads();  // this tile's factor table is complete
+                const Cx *vc = vec + c * NVP;
+                const Real s = Real(a.tw_scale);  // a power of two: exact
+#pragma unroll
+                for (int r = 0; r < E; ++r) {
+                    const int k1 = B::last_freq(tp, r);
+                    v[r] = cscale(cmulc(cmulc(v[r], vc[k1 & 63]), vc[64 + (k1 >> 6)]), s);
+                }
+            }
             B::inverse(sm, tp, v, tw);
         } else {
 #pragma unroll
@@ -431,7 +459,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_TRANS) {
 #pragma unroll
             for (int r = 0; r < E; ++r)
-                v[r] = apply_trans(a.tr, (int64_t(B::first_pos(tp, r)) << log_n2) + col, v[r]);
+                v[r] = apply_trans(a.tr, base + (int64_t(B::first_pos(tp, r)) << log_n2) + col, v[r]);
         }
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
@@ -506,7 +534,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
-    const int64_t tiles = (int64_t(1) << a.log_n2) / C;
+    const int64_t tiles = (a.n >> LG) / C;
     k<<<dim3(unsigned(tiles < cap ? tiles : cap)), dim3(B::NT), smem, s>>>(a);
     count_launch();
     return cudaGetLastError();
