@@ -1,21 +1,33 @@
 #!/usr/bin/env python
 """Benchmark: split-step wavefront propagation throughput on B200.
 
-Workload (one bench step): the three-grating Talbot-Lau interferometer at
-N = 2^24 complex128 (dx = 2 nm), 32 energies 20-70 keV weighted by a filtered
-Kramers spectrum, G2 stepped over 8 phase steps -> 102 split steps per energy,
-3264 split steps per bench step, detector intensity accumulated in FP64.
-Inputs are seeded synthetic (plane-wave illumination, tabulated materials).
+Default workload (one bench step): the three-grating Talbot-Lau
+interferometer at N = 2^24 complex128 (dx = 2 nm), 32 energies 20-70 keV
+weighted by a filtered Kramers spectrum, G2 stepped over 8 phase steps ->
+102 split steps per energy, 3264 split steps per bench step, detector
+intensity accumulated in FP64. Inputs are seeded synthetic (plane-wave
+illumination, tabulated materials).
+
+Other workloads (--workload):
+  batched       128 energies on fields of 2^20..2^25 samples over one
+                window (one field length per group of ~21 energies, groups on
+                separate streams), complex64 by default
+  thick_sample  the interferometer with a 200-slice cracked aluminium
+                cylinder between G1 and G2, N = 2^26 (--energies per step)
+  large_field   the interferometer on 2^31 complex64 / 2^30 complex128 samples
+--compare-fp64 adds the detector error of a complex64 run against the
+complex128 run of the same step (rel-L2 and max-abs / max).
 
 Metric: propagated complex samples * split steps per second (whole job, all
 ranks). One split step = one transmission + FFT + transfer function + iFFT
 of the reference's schedule (big-wave/wavesim.py:84-298).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rsw|reference]
+                    [--workload talbot_lau|batched|thick_sample|large_field]
 
 Multi-GPU (torchrun, one rank per GPU): weak scaling, each rank runs its own
-32 energies of a 32*N-energy spectrum; the FP64 detector accumulators are
-summed with one NCCL all-reduce per step.
+share of an N-times larger energy list (longest-processing-time sharding);
+the FP64 detector accumulators are summed with one NCCL all-reduce per step.
 """
 
 from __future__ import annotations
@@ -47,12 +59,27 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rsw", choices=["rsw", "reference"])
-    ap.add_argument("--dtype", default="c16", choices=["c16", "c8"])
-    ap.add_argument("--logn", type=int, default=24)
-    ap.add_argument("--energies", type=int, default=32)
+    ap.add_argument("--workload", default="talbot_lau",
+                    choices=["talbot_lau", "batched", "thick_sample", "large_field"])
+    ap.add_argument("--dtype", default=None, choices=["c16", "c8"],
+                    help="default: c16 for talbot_lau, c8 otherwise")
+    ap.add_argument("--logn", type=int, default=None, help="field length (talbot_lau 24, thick_sample 26, "
+                    "large_field 31 for c8 / 30 for c16)")
+    ap.add_argument("--energies", type=int, default=None,
+                    help="energies per rank and bench step (talbot_lau 32, batched 128, thick_sample 8, "
+                         "large_field 1)")
+    ap.add_argument("--compare-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.dtype is None:
+        a.dtype = "c16" if a.workload == "talbot_lau" else "c8"
+    if a.logn is None:
+        a.logn = {"talbot_lau": 24, "batched": 25, "thick_sample": 26,
+                  "large_field": 31 if a.dtype == "c8" else 30}[a.workload]
+    if a.energies is None:
+        a.energies = {"talbot_lau": 32, "batched": 128, "thick_sample": 8, "large_field": 1}[a.workload]
+    return a
 
 
 # ------------------------------------------------------------------ helpers
@@ -166,28 +193,78 @@ def reference_arm(args, rank, ws):
     if rank != 0:
         return
     workers = os.cpu_count() or 1
+    lg = min(args.logn, CPU_SAMPLE_MAX_LOGN)
     rates = []
     for i in range(args.warmup + args.steps):
-        r, _ = cpu_split_steps(args.logn, args.dtype, 1, workers)
+        r, _ = cpu_split_steps(lg, args.dtype, 1, workers)
         if i >= args.warmup:
             rates.append(r)
     v = float(np.mean(rates))
-    n = 1 << args.logn
+    n = 1 << lg
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": n / v * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.dtype == "c16" else "f32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.dtype == "c16" else "f32",
         "data": "synthetic",
-        "config": {"workload": f"talbot_lau_3g_N2^{args.logn}_{args.dtype}", "sample": "1 split step per bench step"},
+        "config": {"workload": workload_name(args), "sample": f"1 split step at N=2^{lg} per bench step"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": workers, "kind": "port",
-                         "sample": f"1 grating split step (mask + FFT + transfer + iFFT) at N=2^{args.logn}, "
+                         "sample": f"1 grating split step (mask + FFT + transfer + iFFT) at N=2^{lg}, "
                                    f"scipy.fft workers={workers}"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-# ------------------------------------------------------------------ main
+# ------------------------------------------------------------------ jobs
+CPU_SAMPLE_MAX_LOGN = 24  # the oracle port times its sample at most at 2^24 (host memory and time)
+
+
+def workload_name(args):
+    return {"talbot_lau": f"talbot_lau_3g_N2^{args.logn}_{args.dtype}",
+            "batched": f"batched_128E_N2^20-2^25_{args.dtype}",
+            "thick_sample": f"thick_sample_200slices_N2^{args.logn}_{args.dtype}",
+            "large_field": f"large_field_N2^{args.logn}_{args.dtype}"}[args.workload]
+
+
+def build_groups(args, ws, rank, dtype):
+    """This rank's work: a list of dicts (case, grids, energies, weights, db),
+    one per field length; the energies of all ranks are sharded by cost."""
+    from rave_sim_b200 import workloads
+    from rave_sim_b200.sharding import shard_sources
+
+    items = []  # (group index, energy, weight)
+    groups = []
+    if args.workload == "batched":
+        count = args.energies * ws
+        for g, (case, e, w) in enumerate(workloads.batched_energies(count=count, dtype=dtype)):
+            groups.append({"case": case, "grids": None, "db": workloads.db_table})
+            items += [(g, float(x), float(y)) for x, y in zip(e, w)]
+    else:
+        grids = None
+        db = workloads.db_table
+        if args.workload == "talbot_lau":
+            case = workloads.talbot_lau(n=1 << args.logn, dtype=dtype)
+        elif args.workload == "thick_sample":
+            case, grids = workloads.thick_sample(n=1 << args.logn, dtype=dtype)
+            db = workloads.db_table_sample
+        else:
+            case = workloads.large_field(dtype=dtype, n=1 << args.logn)
+        count = args.energies * ws
+        e, w = workloads.config2_energies(count)
+        groups.append({"case": case, "grids": grids, "db": db})
+        items = [(0, float(x), float(y)) for x, y in zip(e, w)]
+    costs = [float(groups[g]["case"]["sim_params"]["N"]) for g, _, _ in items]
+    mine = shard_sources(costs, ws)[rank]
+    for g in groups:
+        g["energies"], g["weights"] = [], []
+    for i in mine:
+        g, e, w = items[i]
+        groups[g]["energies"].append(e)
+        groups[g]["weights"].append(w)
+    return [g for g in groups if g["energies"]] or groups[:1]
+
+
 def main():
     args = parse()
     rank, ws, local = dist_init(args)
@@ -202,28 +279,37 @@ def main():
     import torch
 
     import rave_sim_b200 as rsw
-    from rave_sim_b200 import workloads
+    from rave_sim_b200.sharding import reduce_detector
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     lib = rsw.load_library()
-    n = 1 << args.logn
-    case = workloads.talbot_lau(n=n, dtype=args.dtype)
-    from rave_sim_b200.sharding import reduce_detector, shard_sources
+    s_bytes = 16 if args.dtype == "c16" else 8
+    groups = build_groups(args, ws, rank, args.dtype)
+    for g in groups:
+        g["sim"] = rsw.Simulation(g["case"], grids=g["grids"], dtype=args.dtype)
+        g["n"] = int(g["case"]["sim_params"]["N"])
+    main_stream = torch.cuda.current_stream()
+    for g in groups:
+        g["stream"] = torch.cuda.Stream() if len(groups) > 1 else main_stream
+    sim0 = groups[0]["sim"]
+    acc = torch.zeros((sim0.nr_phase_steps, sim0.n_pix), dtype=torch.float64, device=dev)
+    accs = [torch.zeros_like(acc) for _ in groups]
 
-    all_e, all_w = workloads.config2_energies(args.energies * ws)
-    mine = shard_sources([1.0] * len(all_e), ws)[rank]  # equal cost: same N and schedule per energy
-    my_e, my_w = all_e[mine], all_w[mine]
-    sim = rsw.Simulation(case, dtype=args.dtype)
-    acc = torch.zeros((sim.nr_phase_steps, sim.n_pix), dtype=torch.float64, device=dev)
-    stream = torch.cuda.current_stream()
-
-    def run_step(source, field=None):
-        sim.reset()
-        for e, w in zip(my_e, my_w):
-            sim.run_source(energy=float(e), db_table=workloads.db_table(float(e)), source=source,
-                           weight=float(w), field=field)
-        sim.detected_device(acc)
+    def run_step(fields=None):
+        for i, g in enumerate(groups):
+            g["stream"].wait_stream(main_stream)
+            with torch.cuda.stream(g["stream"]):
+                sim = g["sim"]
+                sim.reset()
+                src = g["case"]["source"] if fields is None else {"type": "vector", "z": g["case"]["source"]["z"]}
+                f = None if fields is None else fields[i]
+                for e, w in zip(g["energies"], g["weights"]):
+                    sim.run_source(energy=e, db_table=g["db"](e), source=src, weight=w, field=f)
+                sim.detected_device(accs[i])
+        for g in groups:
+            main_stream.wait_stream(g["stream"])
+        torch.sum(torch.stack(accs), dim=0, out=acc)
         reduce_detector(acc)
 
     def barrier():
@@ -243,12 +329,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    plane = case["source"]
-    s0 = sim.split_steps
-    run_step(plane)
-    steps_per_bench_step = sim.split_steps - s0
+    s0 = [g["sim"].split_steps for g in groups]
+    run_step()
+    torch.cuda.synchronize()
+    steps_g = [g["sim"].split_steps - a for g, a in zip(groups, s0)]
+    samples_step = float(sum(g["n"] * k for g, k in zip(groups, steps_g)))
     for _ in range(args.warmup - 1):
-        run_step(plane)
+        run_step()
 
     # ---- timed region (device resident)
     gpu_id = str(getattr(torch.cuda.get_device_properties(dev), "uuid", local))
@@ -259,97 +346,140 @@ def main():
     l0 = lib.rsw_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_wall = time.perf_counter()
-    ev0.record(stream)
+    ev0.record(main_stream)
     for _ in range(args.steps):
-        run_step(plane)
-    ev1.record(stream)
+        run_step()
+    ev1.record(main_stream)
     barrier()
     t_wall = time.perf_counter() - t_wall
     launches = lib.rsw_launch_count() - l0
     clk = clocks.stop()
     ms = max_over_ranks(ev0.elapsed_time(ev1)) / args.steps
-    total_samples = float(n) * steps_per_bench_step * ws
+    total_samples = samples_step * ws  # weak scaling: every rank runs an equal share
     value = total_samples / (ms * 1e-3)
 
-    # ---- end to end through the public API with host buffers
-    npd = np.complex128 if args.dtype == "c16" else np.complex64
-    h_field = torch.from_numpy(np.ones(n, npd)).pin_memory()
-    d_field = torch.empty(n, dtype=h_field.dtype, device=dev)
-    h_out = torch.empty((sim.nr_phase_steps, sim.n_pix), dtype=torch.float64).pin_memory()
-    vec = {"type": "vector", "z": plane["z"]}
-
-    def e2e_step():
-        d_field.copy_(h_field, non_blocking=True)
-        run_step(vec, field=d_field)
-        h_out.copy_(acc, non_blocking=True)
-
+    # ---- end to end through the public API with host buffers: each group's
+    # input field uploaded from pinned memory every step (fields above 4 GiB:
+    # plane-wave source, nothing uploaded), detector read back
     e2e_ms = e2e_value = None
+    h2d = 0
+    h_out = torch.empty_like(acc, device="cpu").pin_memory()
     if not args.no_e2e:
+        npd = np.complex128 if args.dtype == "c16" else np.complex64
+        upload = all(g["n"] * s_bytes <= (4 << 30) for g in groups)
+        if upload:
+            h_fields = [torch.from_numpy(np.ones(g["n"], npd)).pin_memory() for g in groups]
+            d_fields = [torch.empty(g["n"], dtype=h.dtype, device=dev) for g, h in zip(groups, h_fields)]
+            h2d = sum(g["n"] * s_bytes for g in groups)
+
+        def e2e_step():
+            if upload:
+                for d, h in zip(d_fields, h_fields):
+                    d.copy_(h, non_blocking=True)
+            run_step(d_fields if upload else None)
+            h_out.copy_(acc, non_blocking=True)
+
         e2e_step()
         barrier()
         ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e2e_steps = max(1, min(args.steps, 2))
-        ev2.record(stream)
+        ev2.record(main_stream)
         for _ in range(e2e_steps):
             e2e_step()
-        ev3.record(stream)
+        ev3.record(main_stream)
         barrier()
         e2e_ms = max_over_ranks(ev2.elapsed_time(ev3)) / e2e_steps
         e2e_value = total_samples / (e2e_ms * 1e-3)
 
-    # ---- per-kernel device time (CUDA events on the launch stream), one energy
+    # ---- per-kernel device time (CUDA events on the launch stream), one
+    # energy of the largest field
+    gd = max(groups, key=lambda g: g["n"])
+    n = gd["n"]
+    sim = gd["sim"]
     sim.set_timing(True)
-    sim.run_source(energy=float(my_e[0]), db_table=workloads.db_table(float(my_e[0])), source=plane, weight=0.0)
+    e = gd["energies"][0]
+    sim.run_source(energy=e, db_table=gd["db"](e), source=gd["case"]["source"], weight=0.0)
     kinds = {}
-    for k, name in ((0, "row_pass"), (1, "col_pass"), (2, "detect")):
+    for k, name in ((0, "row_pass"), (1, "col_pass"), (2, "detect"), (3, "mid_pass")):
         t, cnt = sim.timing(k)
-        kinds[name] = {"ms_total": t, "launches": cnt, "ms_avg": t / cnt if cnt else None}
+        if cnt or k < 3:
+            kinds[name] = {"ms_total": t, "launches": cnt, "ms_avg": t / cnt if cnt else None}
     sim.set_timing(False)
-    s_bytes = 16 if args.dtype == "c16" else 8
-    dom = max(("row_pass", "col_pass"), key=lambda k: kinds[k]["ms_total"])
+    passes = [k for k in ("row_pass", "col_pass", "mid_pass") if k in kinds and kinds[k]["launches"]]
+    dom = max(passes, key=lambda k: kinds[k]["ms_total"])
     avg_ms = kinds[dom]["ms_avg"]
     algo_bytes = 2.0 * n * s_bytes  # read + write of the field per pass launch
     peak, peak_kind = measured_peak_hbm()
     achieved = algo_bytes / (avg_ms * 1e-3) / 1e9
-    for k in ("row_pass", "col_pass"):
-        if kinds[k]["ms_avg"]:
-            kinds[k]["GBps"] = algo_bytes / (kinds[k]["ms_avg"] * 1e-3) / 1e9
+    for k in passes:
+        kinds[k]["GBps"] = algo_bytes / (kinds[k]["ms_avg"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": algo_bytes,
-                "traffic": ncu_traffic(dom, args.dtype, args.logn), "kernels": kinds}
+                "traffic": ncu_traffic(dom, args.dtype, int(round(math.log2(n)))), "kernels": kinds}
+
+    # ---- mixed precision against the complex128 run of the same step
+    precision = None
+    if args.compare_fp64 and args.dtype == "c8":
+        ref = torch.zeros_like(acc)
+        for g, a in zip(groups, accs):
+            s16 = rsw.Simulation(g["case"], grids=g["grids"], dtype="c16")
+            s16.reset()
+            for e, w in zip(g["energies"], g["weights"]):
+                s16.run_source(energy=e, db_table=g["db"](e), source=g["case"]["source"], weight=w)
+            ref += s16.detected_device()
+            s16.close()
+        run_step()
+        reduce_detector(ref)
+        d = (acc - ref).double()
+        precision = {"rel_l2": float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(ref)),
+                     "max_abs_over_max": float(d.abs().max() / ref.abs().max()),
+                     "reference": "complex128 run of the same energies and phase steps"}
 
     # ---- CPU baseline (rank 0, N=1): oracle port on a bounded sample
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         k = 3
-        v, dt = cpu_split_steps(args.logn, args.dtype, k, 1)
+        lg = min(int(round(math.log2(n))), CPU_SAMPLE_MAX_LOGN)
+        v, dt = cpu_split_steps(lg, args.dtype, k, 1)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{k} grating split steps (mask + FFT + transfer + iFFT) at N=2^{args.logn} "
+               "sample": f"{k} grating split steps (mask + FFT + transfer + iFFT) at N=2^{lg} "
                          f"{args.dtype}, FP64 numpy/scipy oracle, 1 thread, {dt:.1f} s"}
 
     if rank == 0:
+        cfg = {"workload": workload_name(args),
+               "fields": [{"n": g["n"], "energies": len(g["energies"]), "split_steps": k}
+                          for g, k in zip(groups, steps_g)],
+               "phase_steps": sim0.nr_phase_steps,
+               "split_steps_per_bench_step": int(sum(steps_g)) * ws,
+               "l2_policy": "inputs larger than L2" if n * s_bytes > (126 << 20) else
+                            "field smaller than L2 (no flush)",
+               "parallelism": f"dp{ws} (energies sharded, detector all-reduce)"}
+        if args.workload == "talbot_lau":
+            cfg.update({"n": n, "energies_per_rank": len(gd["energies"]), "field_bytes": n * s_bytes,
+                        "l2_policy": "inputs larger than L2 (field 2^24 c128 = 256 MiB)"
+                        if n * s_bytes > (126 << 20) else "field smaller than L2 (no flush)"})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.dtype == "c16" else "f32+f64",
-            "data": "synthetic (seeded plane wave, tabulated gratings)",
-            "config": {"workload": f"talbot_lau_3g_N2^{args.logn}_{args.dtype}",
-                       "n": n, "energies_per_rank": len(my_e), "phase_steps": sim.nr_phase_steps,
-                       "split_steps_per_bench_step": steps_per_bench_step * ws,
-                       "field_bytes": n * s_bytes, "l2_policy": "inputs larger than L2 (field 2^24 c128 = 256 MiB)",
-                       "parallelism": f"dp{ws} (energies sharded, detector all-reduce)"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * s_bytes,
-                    "d2h_bytes_per_step": sim.nr_phase_steps * sim.n_pix * 8, "ms_per_step": e2e_ms},
+            "data": "synthetic (seeded plane wave, tabulated gratings"
+                    + (", seeded cracked-cylinder phantom)" if args.workload == "thick_sample" else ")"),
+            "config": cfg,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": int(acc.numel()) * 8, "ms_per_step": e2e_ms},
             "gpu_launches": int(launches),
             "wall_s": t_wall,
             "clocks": clk,
             "roofline": roofline,
             "cpu_baseline": cpu,
         }
+        if precision is not None:
+            line["precision"] = precision
         print(json.dumps(line), flush=True)
-    sim.close()
+    for g in groups:
+        g["sim"].close()
     if ws > 1:
         import torch.distributed as dist
 

@@ -50,8 +50,8 @@ struct PropArgs {
     double rdx;         // 1.0 / dx
     int64_t cut_lo, cut_hi;  // zero natural frequency indices k in [cut_lo, cut_hi)
     // Chirp form of the transfer function (two-level plans): phase in turns
-    // G * ks^2, G = c / (2 pi N^2 dx^2) as a double-double, ks = k1 + N1 k2s;
-    // h3 = exp(2 pi i G N1^2 k2s^2) in the row kernel's register order.
+    // G * ks^2, G = c / (2 pi N^2 dx^2) as a double-double, ks = kbase + M k2s;
+    // h3 = exp(2 pi i G M^2 k2s^2) in the row kernel's register order, M = N1 Nb.
     int chirp;
     double g_hi, g_lo;
     const void *h3;

@@ -1,7 +1,12 @@
 """Synthetic Talbot-Lau workloads in the reference's configuration schema.
 
 Seeded, deterministic stand-ins for the benchmark setups of the hot path
-(there is no public dataset for it). Each builder returns a ``case`` dict:
+(there is no public dataset for it): ``single_grating`` (one pi-phase
+grating), ``talbot_lau`` (three-grating interferometer, 32 energies x 8
+phase steps), ``batched_energies`` (the interferometer over 128 energies with
+per-energy field lengths 2^20..2^25), ``thick_sample`` (a 200-slice cracked
+aluminium cylinder between G1 and G2) and ``large_field`` (2^30/2^31-sample
+fields). Each builder returns a ``case`` dict:
 the reference's config.yaml keys (``sim_params``, ``elements``, ``dtype``)
 plus ``cutoff_angles`` (computed.yaml) and per-source entries (``energy``,
 ``db`` = subconfig deltabeta table, ``source``).
@@ -105,3 +110,100 @@ def single_grating(n=1 << 20, dx=2e-9, dtype="c16", nr_steps=10):
         "energy": E_REF,
         "db": [[SI, list(SI_46)]],
     }
+
+
+# ---------------------------------------------------------------- batched
+def batched_energies(count=128, e_min=20000.0, e_max=70000.0, log_min=20, log_max=25, window=None,
+                     dtype="c8", nr_steps=10, phase_steps=8):
+    """Benchmark config 3: the interferometer over ``count`` energies, energy
+    j (ascending) on a field of N_j = 2^(log_min + floor((log_max - log_min + 1) j / count))
+    samples over a fixed window (default 2^log_max * 1 nm), dx_j = window / N_j.
+    Returns a list of groups ``(case, energies, weights)``, one per field
+    length; ``case["energy"]``/``case["db"]`` are per-energy (see ``db_table``)."""
+    levels = log_max - log_min + 1
+    win = window if window is not None else float(1 << log_max) * 1e-9
+    e = np.linspace(e_min, e_max, count)
+    w = kramers_weights(e, e_max)
+    groups = []
+    for lg in range(log_min, log_max + 1):
+        idx = [j for j in range(count) if log_min + (levels * j) // count == lg]
+        if not idx:
+            continue
+        n = 1 << lg
+        case = talbot_lau(n=n, dx=win / n, dtype=dtype, nr_steps=nr_steps, phase_steps=phase_steps)
+        groups.append((case, e[idx], w[idx]))
+    return groups
+
+
+# ------------------------------------------------------------ thick sample
+AL = ["Al", 2.70]
+# delta of aluminium at 46 keV from silicon's by the electron-density ratio
+# (rho Z / A: Al 2.70 * 13 / 26.982, Si 2.34 * 14 / 28.086)
+AL_DELTA_46 = SI_46[0] * (2.70 * 13 / 26.982) / (2.34 * 14 / 28.086)
+
+
+def al_deltabeta(energy):
+    """delta ~ E^-2 from the 46 keV value; beta = mu wl / (4 pi) from the
+    tabulated attenuation."""
+    wl = wavelength_from_energy(energy)
+    r = E_REF / energy
+    return [AL_DELTA_46 * r * r, al_mu_per_cm(energy) * 100.0 * wl / (4 * math.pi)]
+
+
+def db_table_sample(energy):
+    return db_table(energy) + [[AL, al_deltabeta(energy)]]
+
+
+def cracked_cylinder(rows=200, cols=4000, psz=10e-6, psx=0.5e-6, diameter=2e-3, cracks=50,
+                     axis_range=(1e-6, 20e-6), seed=4):
+    """int8 grid [rows, cols] of a z-x section through an aluminium cylinder
+    (material 1) with ``cracks`` elliptical air cracks (material 0). Crack
+    centres are uniform inside the disk, semi-axes uniform in ``axis_range``,
+    orientation uniform in [0, pi); each cell is classified by its centre."""
+    rng = np.random.default_rng(seed)
+    rad = diameter / 2
+    zc = (np.arange(rows) + 0.5) * psz - rows * psz / 2
+    xc = (np.arange(cols) + 0.5) * psx - cols * psx / 2
+    Z, X = np.meshgrid(zc, xc, indexing="ij")
+    grid = (Z * Z + X * X <= rad * rad).astype(np.int8)
+    for _ in range(cracks):
+        while True:
+            cz, cx = rng.uniform(-rad, rad, 2)
+            if cz * cz + cx * cx <= rad * rad:
+                break
+        a, b = rng.uniform(axis_range[0], axis_range[1], 2)
+        th = rng.uniform(0.0, math.pi)
+        dz, dx = Z - cz, X - cx
+        u = dz * math.cos(th) + dx * math.sin(th)
+        v = -dz * math.sin(th) + dx * math.cos(th)
+        grid[(u / a) ** 2 + (v / b) ** 2 <= 1.0] = 0
+    return grid
+
+
+def thick_sample(n=1 << 26, dx=50e-9, dtype="c8", nr_steps=10, phase_steps=8, rows=200, cols=4000,
+                 psz=10e-6, psx=0.5e-6, gap=1e-3, seed=4):
+    """Benchmark config 4: the interferometer with a ``sample`` element (the
+    cracked cylinder of ``cracked_cylinder``) starting ``gap`` after the G1
+    exit. Returns (case, grids) with the grid under element index 2; the
+    deltabeta table of an energy is ``db_table_sample``."""
+    case = talbot_lau(n=n, dx=dx, dtype=dtype, nr_steps=nr_steps, phase_steps=phase_steps)
+    g1 = case["elements"][1]
+    z0 = g1["z_start"] + g1["thickness"] + gap
+    grid = cracked_cylinder(rows, cols, psz, psx, seed=seed)
+    sample = {"type": "sample", "z_start": z0, "pixel_size_x": psx, "pixel_size_z": psz,
+              "grid_path": "cracked_cylinder.npy", "materials": [AL], "x_positions": [0.0]}
+    case["elements"].insert(2, sample)
+    case["cutoff_angles"] = [math.pi / 2] * (len(case["elements"]) + 1)
+    case["db"] = db_table_sample(E_REF)
+    return case, {2: grid}
+
+
+# ------------------------------------------------------------- large field
+def large_field(dtype="c8", n=None, dx=5e-9, nr_steps=10, phase_steps=8, pixel_size=75e-6,
+                detector_size=9.6e-3):
+    """Benchmark config 5: the interferometer on one large field, 2^31
+    complex64 or 2^30 complex128 samples at 5 nm, 75 um detector pixels."""
+    if n is None:
+        n = 1 << (31 if dtype == "c8" else 30)
+    return talbot_lau(n=n, dx=dx, dtype=dtype, nr_steps=nr_steps, phase_steps=phase_steps,
+                      detector_size=detector_size, pixel_size=pixel_size)
