@@ -152,6 +152,21 @@ rsw_status rsw_detector_geometry(int64_t n, double dx, double detector_size,
                                  double pixel_size_x, double z, int64_t *n_pix,
                                  int64_t *bounds, double *cosv, double *rv);
 
+/* ------------------------------------------------------ signal retrieval
+ * Phase-stepping signal retrieval on the device: signal_retrieval_least_squares
+ * of the reference's crack-simulation notebook (notebooks/Crack_simulation.ipynb,
+ * cell 4), applied to detector output. d_data: [nsteps][n_pix] FP64, the layout
+ * of detected.npy and rsw_sim_read. Phase steps phi_k = k * (2 pi nsteps /
+ * period) / nsteps (np.linspace(0, 2 pi nsteps / period, nsteps, endpoint=False));
+ * period = nsteps covers one fringe period. Per pixel, the least-squares fit
+ * I_k = a sin(phi_k) + b cos(phi_k) + c gives
+ *   d_abs = nsteps * c, d_phase = -atan2(a, b), d_vis = sqrt(a^2 + b^2) / c,
+ *   d_chi2 = sum_k (I_k - fit_k)^2 (the notebook returns the mean over pixels).
+ * Any output may be NULL. 3 <= nsteps <= 64; allocates nothing. */
+rsw_status rsw_signal_retrieval(const double *d_data, int64_t n_pix, int nsteps, double period,
+                                double *d_abs, double *d_phase, double *d_vis, double *d_chi2,
+                                void *stream);
+
 /* ---------------------------------------------------------- simulations
  * A whole per-source schedule (big-wave/wavesim.py:84-298, fast-wave
  * run_simulation_inner, src/simulation.cpp:375-549) run on the fused engine:

@@ -6,5 +6,7 @@ The CUDA engine lives in ``librsw.so`` (built in-tree from ``csrc/`` by
 
 from ._lib import RswError, load as load_library  # noqa: F401
 from .engine import Plan, Simulation, run_case, wavelength_from_energy  # noqa: F401
+from .retrieval import dark_field, signal_retrieval_least_squares  # noqa: F401
 
-__all__ = ["Plan", "Simulation", "run_case", "wavelength_from_energy", "RswError", "load_library"]
+__all__ = ["Plan", "Simulation", "run_case", "wavelength_from_energy", "RswError", "load_library",
+           "signal_retrieval_least_squares", "dark_field"]

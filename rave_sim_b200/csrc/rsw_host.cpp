@@ -33,6 +33,8 @@ cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log
 cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
                                    bool dbl, cudaStream_t s);
 cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cudaStream_t s);
+cudaError_t launch_retrieval(const double *data, int64_t n_pix, const RetrievalArgs &r, double *dabs, double *dphase,
+                             double *dvis, double *chi2, cudaStream_t s);
 cudaError_t launch_copy(const void *in, void *out, int64_t n, bool dbl, cudaStream_t s);
 cudaError_t launch_point_source(void *u, int64_t n, double dx, double w, double z, double x_src, bool dbl,
                                 cudaStream_t s);
@@ -956,6 +958,52 @@ rsw_status rsw_detector_geometry(int64_t n, double dx, double det, double psx, d
     if (bounds) std::copy(g.bounds.begin(), g.bounds.end(), bounds);
     if (cosv) std::copy(g.cosv.begin(), g.cosv.end(), cosv);
     if (rv) std::copy(g.rv.begin(), g.rv.end(), rv);
+    return RSW_OK;
+}
+
+rsw_status rsw_signal_retrieval(const double *d_data, int64_t n_pix, int nsteps, double period, double *d_abs,
+                                double *d_phase, double *d_vis, double *d_chi2, void *stream) {
+    if (!d_data) return fail(RSW_ERR_INVALID, "d_data is NULL");
+    if (n_pix < 0) return fail(RSW_ERR_INVALID, "n_pix < 0");
+    if (nsteps < 3 || nsteps > RSW_RETRIEVAL_MAX)
+        return fail(RSW_ERR_INVALID, "nsteps = %d: need 3 <= nsteps <= %d", nsteps, RSW_RETRIEVAL_MAX);
+    if (!(period > 0)) return fail(RSW_ERR_INVALID, "period must be positive");
+    // design matrix [sin, cos, 1] at phi_k = k * step, step = (2 pi nsteps / period) / nsteps
+    RetrievalArgs r{};
+    r.k = nsteps;
+    const double step = (2.0 * M_PI * double(nsteps) / period) / double(nsteps);
+    long double g[3][3] = {{0}};
+    for (int k = 0; k < nsteps; ++k) {
+        const double phi = double(k) * step;
+        r.sn[k] = std::sin(phi);
+        r.cs[k] = std::cos(phi);
+        const long double m[3] = {r.sn[k], r.cs[k], 1.0L};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) g[i][j] += m[i] * m[j];
+    }
+    // pseudo-inverse (M^T M)^-1 M^T from the adjugate of the 3 x 3 Gram matrix
+    long double inv[3][3];
+    inv[0][0] = g[1][1] * g[2][2] - g[1][2] * g[2][1];
+    inv[0][1] = g[0][2] * g[2][1] - g[0][1] * g[2][2];
+    inv[0][2] = g[0][1] * g[1][2] - g[0][2] * g[1][1];
+    inv[1][0] = g[1][2] * g[2][0] - g[1][0] * g[2][2];
+    inv[1][1] = g[0][0] * g[2][2] - g[0][2] * g[2][0];
+    inv[1][2] = g[0][2] * g[1][0] - g[0][0] * g[1][2];
+    inv[2][0] = g[1][0] * g[2][1] - g[1][1] * g[2][0];
+    inv[2][1] = g[0][1] * g[2][0] - g[0][0] * g[2][1];
+    inv[2][2] = g[0][0] * g[1][1] - g[0][1] * g[1][0];
+    const long double det = g[0][0] * inv[0][0] + g[0][1] * inv[1][0] + g[0][2] * inv[2][0];
+    if (!(std::fabs(double(det)) > 1e-12)) return fail(RSW_ERR_INVALID, "phase steps do not determine the fit");
+    for (int k = 0; k < nsteps; ++k) {
+        const long double m[3] = {r.sn[k], r.cs[k], 1.0L};
+        for (int i = 0; i < 3; ++i) {
+            long double acc = 0;
+            for (int j = 0; j < 3; ++j) acc += inv[i][j] * m[j];
+            r.p[i * RSW_RETRIEVAL_MAX + k] = double(acc / det);
+        }
+    }
+    cudaError_t e = launch_retrieval(d_data, n_pix, r, d_abs, d_phase, d_vis, d_chi2, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "signal retrieval: %s", cudaGetErrorString(e));
     return RSW_OK;
 }
 

@@ -96,4 +96,14 @@ struct PassArgs {
     PropArgs pr;
 };
 
+// Phase-step signal retrieval: the 3 x K pseudo-inverse of [sin phi_k,
+// cos phi_k, 1] (rows a, b, c at stride RSW_RETRIEVAL_MAX) and the design
+// matrix columns for the residuals.
+constexpr int RSW_RETRIEVAL_MAX = 64;
+struct RetrievalArgs {
+    int k;
+    double p[3 * RSW_RETRIEVAL_MAX];
+    double sn[RSW_RETRIEVAL_MAX], cs[RSW_RETRIEVAL_MAX];
+};
+
 }  // namespace rsw

@@ -200,3 +200,44 @@ cudaError_t launch_fill_ones(void *u, int64_t n, bool dbl, cudaStream_t s) {
     return cudaGetLastError();
 }
 }  // namespace rsw
+
+namespace rsw {
+// Phase-step signal retrieval: per pixel j the least-squares fit of
+// I_k = a sin(phi_k) + b cos(phi_k) + c over the K phase steps, as
+// (a, b, c) = P I with the 3 x K pseudo-inverse P of [sin, cos, 1] (built on
+// the host); outputs as signal_retrieval_least_squares of the reference's
+// crack-simulation notebook: abs = K c, phase = -atan2(a, b),
+// vis = sqrt(a^2 + b^2) / c, chi2 = squared residual norm.
+__global__ void retrieval_kernel(const double *__restrict__ data, int64_t n_pix, RetrievalArgs r,
+                                 double *__restrict__ dabs, double *__restrict__ dphase,
+                                 double *__restrict__ dvis, double *__restrict__ chi2) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n_pix; j += stride) {
+        double a = 0.0, b = 0.0, c = 0.0;
+        for (int k = 0; k < r.k; ++k) {
+            const double v = data[int64_t(k) * n_pix + j];
+            a = fma(r.p[k], v, a);
+            b = fma(r.p[RSW_RETRIEVAL_MAX + k], v, b);
+            c = fma(r.p[2 * RSW_RETRIEVAL_MAX + k], v, c);
+        }
+        if (chi2) {
+            double e2 = 0.0;
+            for (int k = 0; k < r.k; ++k) {
+                const double e = data[int64_t(k) * n_pix + j] - (a * r.sn[k] + b * r.cs[k] + c);
+                e2 = fma(e, e, e2);
+            }
+            chi2[j] = e2;
+        }
+        if (dabs) dabs[j] = c * double(r.k);
+        if (dphase) dphase[j] = -atan2(a, b);
+        if (dvis) dvis[j] = sqrt(a * a + b * b) / c;
+    }
+}
+cudaError_t launch_retrieval(const double *data, int64_t n_pix, const RetrievalArgs &r, double *dabs, double *dphase,
+                             double *dvis, double *chi2, cudaStream_t s) {
+    if (n_pix <= 0) return cudaSuccess;
+    ++g_launches;
+    retrieval_kernel<<<grid_for(n_pix, 256), 256, 0, s>>>(data, n_pix, r, dabs, dphase, dvis, chi2);
+    return cudaGetLastError();
+}
+}  // namespace rsw
