@@ -59,6 +59,11 @@ template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
 template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) {
     return mk(a.x * s, a.y * s);
 }
+// complex64: packed FP32x2 arithmetic (one instruction per complex add, sub
+// or real scale); b * -1 + a rounds exactly like a - b
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 
 __host__ __device__ constexpr int brev_bits(int q, int bits) {
     int r = 0;
