@@ -257,6 +257,20 @@ rsw_status rsw_sim_final_field(rsw_sim sim, void *d_dst, void *stream);
 rsw_status rsw_sim_set_timing(rsw_sim sim, int enable);
 rsw_status rsw_sim_timing(rsw_sim sim, int kind, double *ms, int64_t *launches);
 
+/* History recording (big-wave/history.py:43-135, the reference's --history_dz):
+ * with history_dz > 0, each following rsw_sim_run records detector images
+ * (square_and_downsample at the image's z) on its first phase-step pass:
+ * the analytic point-source intensity at np.arange(0, z_first, history_dz)[1:],
+ * free-space gaps sampled every history_dz (each point propagated from the
+ * gap's start, the last moved to the gap end when closer than history_dz/2),
+ * after every grating sub-step and before every sample row. 0 disables.
+ * rsw_sim_history copies the images of the last run as [n_pix][n_entries]
+ * (np.stack(entries, axis=-1)) and their z to host memory; NULL outputs are
+ * skipped; it synchronises. */
+rsw_status rsw_sim_set_history(rsw_sim sim, double history_dz);
+rsw_status rsw_sim_history(rsw_sim sim, double *h_history, double *h_z, int64_t *n_entries,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -174,10 +174,11 @@ def _lookup_db(db_table, mat):
     return np.complex128(cands[0][1])
 
 
-def apply_grating(u, U, sim, el, db_table, cutoff, step_idx, dba=False):
+def apply_grating(u, U, sim, el, db_table, cutoff, step_idx, dba=False, hist=None):
     """``Grating.apply`` / ``DBAGrating.apply`` (big-wave/optical_element.py:134-206,
     :247-319): ``nr_steps`` x [binary mask multiply, propagate(thickness/nr_steps)],
-    then the substrate as a scalar factor and one more propagate."""
+    then the substrate as a scalar factor and one more propagate. ``hist``
+    (a list) receives the detector image after every sub-step (:181-186)."""
     z_step = el["thickness"] / el["nr_steps"]
     fa = material_factor(_lookup_db(db_table, el.get("mat_a")), z_step, sim.wl)
     fb = material_factor(_lookup_db(db_table, el.get("mat_b")), z_step, sim.wl)
@@ -193,6 +194,9 @@ def apply_grating(u, U, sim, el, db_table, cutoff, step_idx, dba=False):
             fn = lambda s, c: grating_mask_chunk(sim.dx, s, c, el["pitch"], dc, x_pos)
         u = _apply_binary(u, sim, fn, fa, fb)
         u, U = propagate(u, U, sim, z_step, cutoff)
+        if hist is not None:
+            z = el["z_start"] + (i + 1) * z_step
+            hist.append((square_and_downsample(u, sim, z), z))
     t_sub = el["substrate_thickness"]
     if t_sub > 0:
         fs = material_factor(_lookup_db(db_table, el.get("mat_substrate")), t_sub, sim.wl)
@@ -206,16 +210,20 @@ def sample_row_coordinates(rowlen, psx, x_pos):
     return np.arange(rowlen) * psx + x_pos - rowlen * psx * 0.5
 
 
-def apply_sample(u, U, sim, el, grid, db_table, cutoff, step_idx):
+def apply_sample(u, U, sim, el, grid, db_table, cutoff, step_idx, hist=None):
     """``Sample.apply`` (big-wave/optical_element.py:432-476): per z-row,
     linear interpolation (``np.interp`` with zero outside) of the row's delta+i*beta
-    at the field's x, ``exp(i 2 pi dz/wl * db)``, then propagate(pixel_size_z)."""
+    at the field's x, ``exp(i 2 pi dz/wl * db)``, then propagate(pixel_size_z).
+    ``hist`` receives the detector image before every row (:447-452)."""
     db_list = np.zeros(len(el["materials"]) + 1, dtype=np.complex128)
     for i, m in enumerate(el["materials"]):
         db_list[i + 1] = _lookup_db(db_table, m)
     psx, psz = el["pixel_size_x"], el["pixel_size_z"]
     row_x = sample_row_coordinates(grid.shape[1], psx, el["x_positions"][step_idx])
     for r in range(grid.shape[0]):
+        if hist is not None:
+            z = el["z_start"] + r * psz
+            hist.append((square_and_downsample(u, sim, z), z))
         row_db = db_list[grid[r, :]]
         out = u.copy()
         for idx, cnt in _chunks(sim.N, sim.chunk_size):
@@ -280,7 +288,50 @@ def make_sim(case) -> Sim:
                chunk_size=int(sp["chunk_size"]))
 
 
-def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False):
+def history_zs(dz, hdz):
+    """z offsets visited by ``propagate_with_history`` (big-wave/history.py:90-97)."""
+    zs = np.arange(0, dz, hdz)
+    if dz - zs[-1] < hdz / 2.0 and len(zs) > 1:
+        zs[-1] = dz
+    else:
+        zs = np.append(zs, [dz])
+    return zs
+
+
+def propagate_with_history(u, U, sim, dz, cutoff, current_z, skip_fft, hist, hdz):
+    """``propagate_with_history`` (big-wave/history.py:67-135): every history
+    point is reached from the spectrum at the start of the gap."""
+    if dz == 0:
+        return u, U
+    if hist is None:
+        return propagate(u, U, sim, dz, cutoff, skip_fft=skip_fft)
+    zs = history_zs(dz, hdz)
+    if not skip_fft:
+        U = spfft.fft(u)
+    U_start = U.copy()
+    for i in range(1, len(zs)):
+        u, U = propagate(u, U_start.copy(), sim, zs[i] - zs[0], cutoff, skip_fft=True)
+        z = zs[i] + current_z
+        hist.append((square_and_downsample(u, sim, z), z))
+    return u, U
+
+
+def analytic_history(hist, zs, x_source, sim, cutoff):
+    """``generate_analytic_history`` (big-wave/history.py:43-64): the point
+    source's intensity on the detector grid at each z, zero outside the cutoff
+    cone."""
+    gradient = cutoff * sim.wl
+    n = sim.detector_size // sim.psx
+    x = (np.arange(n) - n // 2) * sim.psx - x_source
+    for z in zs:
+        angle = np.arctan(x / z)
+        r2 = x ** 2 + z ** 2
+        inten = sim.psx * sim.psy * np.cos(angle) / r2
+        inten[np.abs(x) > gradient * z] = 0
+        hist.append((inten, z))
+
+
+def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False, history_dz=None):
     """``run_simulation`` (big-wave/wavesim.py:84-298) for one source: source
     initialisation, element loop with gap propagation, final gap reusing the
     spectrum (``skip_fft``), detection, then the remaining phase steps
@@ -288,7 +339,10 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False):
 
     ``grids`` maps element index -> int8 grid for sample elements.
     Returns the detector array ``(nr_phase_steps, n_pix)`` (and the final
-    fields of every phase step when ``return_fields``)."""
+    fields of every phase step when ``return_fields``). With ``history_dz``
+    the first pass records the history (big-wave/wavesim.py:153-219) and the
+    result is ``(detector, history (n_pix, entries), z of each entry)``."""
+    hist = [] if history_dz else None
     grids = grids or {}
     sim = make_sim(case)
     elements = [dict(e) for e in case["elements"]]
@@ -299,13 +353,13 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False):
     cut = [np.sin(a) / sim.wl for a in case["cutoff_angles"]]
     z_tol = 1e-8
 
-    def apply(el, u, U, cutoff, step):
+    def apply(el, u, U, cutoff, step, h=None):
         if el["type"] == "grating":
-            return apply_grating(u, U, sim, el, db_table, cutoff, step)
+            return apply_grating(u, U, sim, el, db_table, cutoff, step, hist=h)
         if el["type"] == "dba_grating":
-            return apply_grating(u, U, sim, el, db_table, cutoff, step, dba=True)
+            return apply_grating(u, U, sim, el, db_table, cutoff, step, dba=True, hist=h)
         if el["type"] == "sample":
-            return apply_sample(u, U, sim, el, el["_grid"], db_table, cutoff, step)
+            return apply_sample(u, U, sim, el, el["_grid"], db_table, cutoff, step, hist=h)
         raise ValueError(el["type"])
 
     # source.propagate_to (big-wave/source.py:46-101)
@@ -320,26 +374,29 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False):
         if rng is not None:
             Us[rng[0]:rng[1]] = 0
         u = spfft.ifft(Us)
+        if hist is not None:
+            analytic_history(hist, np.arange(0, z, history_dz)[1:], src["x"], sim, cutoff)
     else:
         u0 = np.ones(sim.N, dtype) if src["type"] == "plane" else np.asarray(src["u"], dtype)
         dz = z - src["z"]
         if dz == 0:
             u = u0.copy()
         else:
-            u, U = propagate(u0, spfft.fft(u0), sim, dz, cutoff, skip_fft=True)
+            u, U = propagate_with_history(u0, spfft.fft(u0), sim, dz, cutoff, src["z"], True, hist, history_dz)
 
     snapshot = None
     for i, el in enumerate(elements):
         if z < el["z_start"]:
-            u, U = propagate(u, U, sim, el["z_start"] - z, cutoff)
+            u, U = propagate_with_history(u, U, sim, el["z_start"] - z, cutoff, z, False, hist, history_dz)
         z = el["z_start"]
         if len(el["x_positions"]) > 1 and snapshot is None:
             snapshot = (z, i, u.copy(), len(el["x_positions"]))
         cutoff = cut[i + 1]
-        u, U = apply(el, u, U, cutoff, 0)
+        u, U = apply(el, u, U, cutoff, 0, hist)
         z = el["z_start"] + element_thickness(el)
     if z < sim.z_detector - z_tol:
-        u, U = propagate(u, U, sim, sim.z_detector - z, cutoff, skip_fft=len(elements) > 0)
+        u, U = propagate_with_history(u, U, sim, sim.z_detector - z, cutoff, z, len(elements) > 0, hist,
+                                      history_dz)
     outs = [square_and_downsample(u, sim, sim.z_detector)]
     fields = [u]
 
@@ -360,6 +417,9 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False):
             outs.append(square_and_downsample(u, sim, sim.z_detector))
             fields.append(u)
     det = np.array(outs)
+    if hist is not None:
+        h = np.stack([e for e, _ in hist], axis=-1) if hist else np.empty((0, 0))
+        return det, h, np.array([z for _, z in hist], dtype=np.float64)
     return (det, fields) if return_fields else det
 
 

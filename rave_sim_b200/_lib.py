@@ -115,6 +115,8 @@ SIGNATURES = {
     "rsw_square_and_downsample": (C.c_int, [_P, _P, _D, _D, _D, _D, _D, _DP, C.POINTER(_I64), _P]),
     "rsw_detector_geometry": (C.c_int, [_I64, _D, _D, _D, _D, C.POINTER(_I64), C.POINTER(_I64), _DP, _DP]),
     "rsw_signal_retrieval": (C.c_int, [_P, _I64, C.c_int, _D, _P, _P, _P, _P, _P]),
+    "rsw_sim_set_history": (C.c_int, [_P, _D]),
+    "rsw_sim_history": (C.c_int, [_P, _DP, _DP, C.POINTER(_I64), _P]),
     "rsw_sim_create": (C.c_int, [C.POINTER(_P), C.POINTER(SimDesc)]),
     "rsw_sim_destroy": (C.c_int, [_P]),
     "rsw_sim_shape": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),

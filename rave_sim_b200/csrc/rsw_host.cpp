@@ -1042,8 +1042,30 @@ struct rsw_sim_s {
     int last_field = -1;
     TimingLog tl;
     int64_t split_steps = 0;
+    // history recording (big-wave/history.py): detector images at the z
+    // points of the first phase-step pass, stored [entry][n_pix] on the device
+    double hist_dz = 0.0;
+    DevBuf hbuf;  // third field buffer: history views and intermediate points
+    DevBuf hist, hist_cos, hist_r;
+    int64_t hist_cap = 0;
+    std::vector<double> hist_z;
     ~rsw_sim_s() { rsw_plan_destroy(plan); }
 };
+
+// z offsets of big-wave's propagate_with_history (big-wave/history.py:90-97):
+// np.arange(0, dz, hdz), the last one moved to dz when closer than hdz / 2,
+// else dz appended
+static std::vector<double> history_zs(double dz, double hdz) {
+    const int64_t len = std::max<int64_t>(int64_t(std::ceil(dz / hdz)), 0);
+    std::vector<double> zs;
+    for (int64_t i = 0; i < len; ++i) zs.push_back(double(i) * hdz);
+    if (zs.empty()) zs.push_back(0.0);
+    if (dz - zs.back() < hdz / 2.0 && zs.size() > 1)
+        zs.back() = dz;
+    else
+        zs.push_back(dz);
+    return zs;
+}
 
 namespace {
 
@@ -1088,22 +1110,30 @@ struct Runner {
         if (cur < 0) return readonly == 0 ? 1 : 0;
         return cur == readonly ? 1 - cur : cur;
     }
+    // field buffers 0 and 1 hold the state; 2 is the history buffer
+    void *bp(int i) const { return i == 2 ? S->hbuf.p : S->buf[i].p; }
 
     rsw_status split_step(const TransArgs &tr, double dz, double cutoff) {
-        const int dst = target();
+        return step_to(tr, dz, cutoff, target(), true);
+    }
+
+    // One split step from the current state into buffer dst; commit = false
+    // leaves the state untouched (history points reached from a gap start).
+    rsw_status step_to(const TransArgs &tr, double dz, double cutoff, int dst, bool commit) {
         PassArgs a = base_args(P);
         a.tr = tr;
         a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0);
         CHECK(chirp_for(a.pr, dz));
+        bool now_mid;
         if (P->log_n1 > 0) {
-            a.in = ones ? nullptr : S->buf[cur].p;
-            a.out = S->buf[dst].p;
+            a.in = ones ? nullptr : bp(cur);
+            a.out = bp(dst);
             a.flags = (mid ? col_inv(P) : 0) | PF_FWD | PF_TW | (tr.kind != TR_NONE ? PF_TRANS : 0) |
                       (ones ? PF_ONES : 0);
             PropArgs keep = a.pr;
             a.pr = PropArgs{};
             CHECK(run_col(P, a, st, &S->tl));
-            a.in = S->buf[dst].p;
+            a.in = bp(dst);
             a.tr.kind = TR_NONE;
             if (P->three()) CHECK(run_mid(P, a, true, st, &S->tl));
             a.pr = keep;
@@ -1114,18 +1144,107 @@ struct Runner {
                 a.pr = PropArgs{};
                 CHECK(run_mid(P, a, false, st, &S->tl));
             }
-            mid = true;
+            now_mid = true;
         } else {
-            a.in = ones ? nullptr : S->buf[cur].p;
-            a.out = S->buf[dst].p;
+            a.in = ones ? nullptr : bp(cur);
+            a.out = bp(dst);
             a.flags = PF_FWD | PF_INV | PF_SCALE | (tr.kind != TR_NONE ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
             CHECK(run_row(P, a, st, &S->tl));
-            mid = false;
+            now_mid = false;
         }
-        cur = dst;
-        ones = false;
+        if (commit) {
+            cur = dst;
+            ones = false;
+            mid = now_mid;
+        }
         ++S->split_steps;
         return RSW_OK;
+    }
+
+    // ---------------------------------------------------------- history
+    bool hist_on = false;
+
+    rsw_status hist_reserve() {
+        const int64_t np = S->geom.n_pix;
+        const int64_t n = int64_t(S->hist_z.size());
+        if (n < S->hist_cap) return RSW_OK;
+        const int64_t cap = std::max<int64_t>(64, 2 * S->hist_cap);
+        const size_t bytes = size_t(cap * std::max<int64_t>(np, 1)) * sizeof(double);
+        DevBuf nb, nc, nr;  // images, and per-entry cos / r of the detector geometry
+        CHECK(nb.alloc(bytes));
+        CHECK(nc.alloc(bytes));
+        CHECK(nr.alloc(bytes));
+        if (n > 0) CU(cudaMemcpyAsync(nb.p, S->hist.p, size_t(n * np) * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CU(cudaStreamSynchronize(st));  // the old buffers are freed below
+        S->hist = std::move(nb);
+        S->hist_cos = std::move(nc);
+        S->hist_r = std::move(nr);
+        S->hist_cap = cap;
+        return RSW_OK;
+    }
+    // detector image of a natural-order field at z (square_and_downsample)
+    rsw_status hist_detect(const void *field, double z) {
+        CHECK(hist_reserve());
+        DetectorGeom g;
+        CHECK(detector_geom(P->n, S->d.dx, S->d.detector_size, S->d.pixel_size_x, z, g));
+        const int64_t off = int64_t(S->hist_z.size()) * S->geom.n_pix;
+        double *cosv = (double *)S->hist_cos.p + off, *rv = (double *)S->hist_r.p + off;
+        // pageable sources: the copies are staged before the calls return
+        CU(cudaMemcpyAsync(cosv, g.cosv.data(), g.cosv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(rv, g.rv.data(), g.rv.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        double *out = (double *)S->hist.p + off;
+        cudaError_t e = launch_detect(field, (const int64_t *)S->bounds.p, cosv, rv, S->geom.n_pix, S->d.dx,
+                                      S->d.pixel_size_y, out, nullptr, nullptr, 1.0, P->dbl(), st);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "history detect: %s", cudaGetErrorString(e));
+        S->hist_z.push_back(z);
+        return RSW_OK;
+    }
+    // history entry of the current state at z
+    rsw_status hist_push(double z) {
+        if (ones) {
+            cudaError_t e = launch_fill_ones(bp(2), P->n, P->dbl(), st);
+            if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "fill: %s", cudaGetErrorString(e));
+            return hist_detect(bp(2), z);
+        }
+        if (mid) {
+            PassArgs a = base_args(P);
+            a.in = bp(cur);
+            a.out = bp(2);
+            a.flags = col_inv(P);
+            CHECK(run_col(P, a, st, &S->tl));
+            return hist_detect(bp(2), z);
+        }
+        return hist_detect(bp(cur), z);
+    }
+    // host-computed entry (analytic point-source history)
+    rsw_status hist_host(const std::vector<double> &img, double z) {
+        CHECK(hist_reserve());
+        double *out = (double *)S->hist.p + int64_t(S->hist_z.size()) * S->geom.n_pix;
+        if (!img.empty()) CU(cudaMemcpyAsync(out, img.data(), img.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        CU(cudaStreamSynchronize(st));  // img is a temporary
+        S->hist_z.push_back(z);
+        return RSW_OK;
+    }
+    // propagate_with_history (big-wave/history.py:67-135): every history point
+    // is reached from the state at the start of the gap; the last one is the
+    // gap's own propagation
+    rsw_status gap(double dz, double cutoff, double z_from) {
+        if (dz == 0.0) return RSW_OK;
+        if (!hist_on) return split_step(TransArgs{}, dz, cutoff);
+        const std::vector<double> zs = history_zs(dz, S->hist_dz);
+        for (size_t i = 1; i + 1 < zs.size(); ++i) {
+            CHECK(step_to(TransArgs{}, zs[i] - zs[0], cutoff, 2, false));
+            if (P->log_n1 > 0) {  // "mid" -> natural, in place
+                PassArgs a = base_args(P);
+                a.in = bp(2);
+                a.out = bp(2);
+                a.flags = col_inv(P);
+                CHECK(run_col(P, a, st, &S->tl));
+            }
+            CHECK(hist_detect(bp(2), zs[i] + z_from));
+        }
+        CHECK(split_step(TransArgs{}, zs.back() - zs[0], cutoff));
+        return hist_push(zs.back() + z_from);
     }
 
     rsw_status finalize() {
@@ -1194,6 +1313,7 @@ struct Runner {
                     tr.chunk_step = (const double *)el.chunk_st[step]->p;
                 }
                 CHECK(split_step(tr, z_step, cutoff));
+                if (hist_on) CHECK(hist_push(e.z_start + double(i + 1) * z_step));
             }
             if (e.substrate_thickness > 0) {
                 const cplx fs = material_factor(m[2].real(), m[2].imag(), e.substrate_thickness, wl);
@@ -1220,6 +1340,7 @@ struct Runner {
         tr.mat_db = (const double2 *)S->mat_db.p + off;
         tr.mat_factor = (const double2 *)S->mat_fac.p + off;
         for (int64_t r = 0; r < e.grid_z; ++r) {
+            if (hist_on) CHECK(hist_push(e.z_start + double(r) * psz));
             tr.row_grid = (const int8_t *)el.grid_dev.p + r * e.grid_x;
             CHECK(split_step(tr, psz, cutoff));
         }
@@ -1389,6 +1510,29 @@ rsw_status rsw_sim_timing(rsw_sim S, int kind, double *ms, int64_t *launches) {
     return RSW_OK;
 }
 
+rsw_status rsw_sim_set_history(rsw_sim S, double history_dz) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    if (!(history_dz >= 0)) return fail(RSW_ERR_INVALID, "history_dz must be >= 0");
+    S->hist_dz = history_dz;
+    return RSW_OK;
+}
+
+rsw_status rsw_sim_history(rsw_sim S, double *h_out, double *h_z, int64_t *n_entries, void *stream) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    const int64_t n = int64_t(S->hist_z.size()), np = S->geom.n_pix;
+    if (n_entries) *n_entries = n;
+    if (h_z) std::copy(S->hist_z.begin(), S->hist_z.end(), h_z);
+    if (h_out && n > 0) {
+        std::vector<double> tmp(size_t(n * np));
+        CU(cudaMemcpyAsync(tmp.data(), S->hist.p, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           (cudaStream_t)stream));
+        CU(cudaStreamSynchronize((cudaStream_t)stream));
+        for (int64_t e = 0; e < n; ++e)
+            for (int64_t j = 0; j < np; ++j) h_out[j * n + e] = tmp[size_t(e * np + j)];
+    }
+    return RSW_OK;
+}
+
 rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
     if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
     if (!(run->energy_ev > 0) && !(run->wavelength_m > 0))
@@ -1437,9 +1581,40 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     R.readonly = -1;
     R.mid = false;
     R.ones = false;
+    s.hist_z.clear();
+    R.hist_on = s.hist_dz > 0;
+    if (R.hist_on) CHECK(s.hbuf.alloc(size_t(s.d.n) * R.P->elem()));
     if (src->type == RSW_SRC_POINT) {
+        // grid_density_check (big-wave/propagation.py:31-45)
+        const double dzs = z - src->z;
+        auto dist_x = [&](double idx) {
+            const double a = (double(s.d.n) / 2.0 - idx) * s.d.dx + std::fabs(src->x);
+            return std::sqrt(a * a + dzs * dzs);
+        };
+        if (!(std::fabs(dist_x(0.0) - dist_x(1.0)) <= R.wl / 2.0))
+            return fail(RSW_ERR_INVALID, "Nyquist not satisfied, dx too large for the point source at dz = %g", dzs);
         CHECK(rsw_point_source(R.P, s.buf[0].p, s.d.dx, R.wl, z - src->z, src->x, stream));
         CHECK(R.split_step(TransArgs{}, 0.0, cutoff));
+        if (R.hist_on) {
+            // generate_analytic_history (big-wave/history.py:43-64) at
+            // np.arange(0, z, hdz)[1:]
+            const double psx = s.d.pixel_size_x, psy = s.d.pixel_size_y;
+            const double nd = py_floordiv(s.d.detector_size, psx);
+            const int64_t npx = int64_t(nd);
+            const double gradient = cutoff * R.wl;
+            const int64_t len = std::max<int64_t>(int64_t(std::ceil(z / s.hist_dz)), 0);
+            for (int64_t k = 1; k < len; ++k) {
+                const double zh = double(k) * s.hist_dz;
+                std::vector<double> img(static_cast<size_t>(npx));
+                for (int64_t j = 0; j < npx; ++j) {
+                    const double x = (double(j) - py_floordiv(nd, 2.0)) * psx - src->x;
+                    const double ang = std::atan(x / zh);
+                    const double r2 = x * x + zh * zh;
+                    img[size_t(j)] = std::fabs(x) > gradient * zh ? 0.0 : psx * psy * std::cos(ang) / r2;
+                }
+                CHECK(R.hist_host(img, zh));
+            }
+        }
     } else if (src->type == RSW_SRC_PLANE || src->type == RSW_SRC_VECTOR) {
         if (src->type == RSW_SRC_PLANE) {
             R.ones = true;
@@ -1452,7 +1627,7 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
             return fail(RSW_ERR_INVALID, "vector source without a field");
         }
         const double dz = z - src->z;
-        if (dz != 0.0) CHECK(R.split_step(TransArgs{}, dz, cutoff));
+        if (dz != 0.0) CHECK(R.gap(dz, cutoff, src->z));
     } else {
         return fail(RSW_ERR_INVALID, "unknown source type %d", src->type);
     }
@@ -1465,7 +1640,7 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     } snap{0, -1, false, false};
     for (int i = 0; i < nel; ++i) {
         const rsw_element &e = s.els[i].d;
-        if (z < e.z_start) CHECK(R.split_step(TransArgs{}, e.z_start - z, cutoff));
+        if (z < e.z_start) CHECK(R.gap(e.z_start - z, cutoff, z));
         z = e.z_start;
         if (i == s.snap_el) {
             snap = Snap{z, R.cur, R.mid, R.ones};
@@ -1475,9 +1650,10 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
         CHECK(R.apply(i, 0, cutoff));
         z = e.z_start + s.els[i].total_thickness();
     }
-    if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, cutoff));
+    if (z < s.d.z_detector - z_tol) CHECK(R.gap(s.d.z_detector - z, cutoff, z));
     CHECK(R.finalize());
     CHECK(R.detect(0, run->weight));
+    R.hist_on = false;  // phase steps from the snapshot record no history (big-wave/wavesim.py:234-237)
 
     // ---- remaining phase steps from the snapshot (big-wave/wavesim.py:238-296)
     for (int64_t step = 1; step < s.nr_phase_steps; ++step) {

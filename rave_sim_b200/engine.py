@@ -371,22 +371,44 @@ class Simulation:
     def set_timing(self, enable: bool):
         L.check(self._lib.rsw_sim_set_timing(self._h, int(bool(enable))))
 
+    def set_history(self, history_dz: Optional[float]):
+        """Record the history of the following runs every ``history_dz``
+        metres (big-wave --history_dz); None or 0 disables."""
+        L.check(self._lib.rsw_sim_set_history(self._h, float(history_dz or 0.0)))
+
+    def history(self):
+        """History of the last run: (images (n_pix, entries), z of each
+        entry) as big-wave's History.get_history() / get_z()."""
+        n = C.c_int64()
+        L.check(self._lib.rsw_sim_history(self._h, None, None, C.byref(n), _stream_ptr()))
+        h = np.zeros((self.n_pix, n.value), dtype=np.float64)
+        z = np.zeros(n.value, dtype=np.float64)
+        L.check(self._lib.rsw_sim_history(self._h, h.ctypes.data_as(L._DP), z.ctypes.data_as(L._DP),
+                                          C.byref(n), _stream_ptr()))
+        return h, z
+
     def timing(self, kind: int):
         ms, n = C.c_double(), C.c_int64()
         L.check(self._lib.rsw_sim_timing(self._h, int(kind), C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
 
-def run_case(case: dict, grids: Optional[dict] = None, dtype=None) -> np.ndarray:
+def run_case(case: dict, grids: Optional[dict] = None, dtype=None, history_dz: Optional[float] = None):
     """Run one source described by a case dict (the oracle's schema: the
     reference config + ``source``, ``energy``, ``db``, ``cutoff_angles``) and
-    return its detector array (nr_phase_steps, n_pix)."""
+    return its detector array (nr_phase_steps, n_pix); with ``history_dz``,
+    (detector, history (n_pix, entries), z of each entry)."""
     sim = Simulation(case, grids=grids, dtype=dtype if dtype is not None else case.get("dtype", "c16"),
                      cutoff_angles=case["cutoff_angles"])
     try:
+        sim.set_history(history_dz)
         sim.reset()
         sim.run_source(energy=case["energy"], db_table=case["db"], source=case["source"],
                        field=case["source"].get("u"))
-        return sim.detected()
+        det = sim.detected()
+        if history_dz:
+            h, z = sim.history()
+            return det, h, z
+        return det
     finally:
         sim.close()

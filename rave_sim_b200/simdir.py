@@ -15,12 +15,13 @@ shape (nr_phase_steps, nr_pixels)) and, with ``save_final_u_vectors`` and no
 phase stepping, ``NNNNNNNN/u_0000.npy``. The command line mirrors fast-wave's
 ``fastwave <sim_dir> -s <idx>`` (fast-wave/main.cpp:18-57):
 
-    python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16]
+    python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16] [--history_dz DZ]
 
-The field stays in GPU memory for the whole source, so ``use_disk_vector`` is
-accepted and ignored. History recording (``--history_dz``) and keypoints are
-not supported: they record intermediate fields, which the fused engine never
-forms.
+With ``--history_dz`` the history of the source is written as
+``history.npy`` (n_pix, entries), ``history_z.npy`` and ``history_x.npy``
+(big-wave/multisim.py:132-141). The field stays in GPU memory for the whole
+source, so ``use_disk_vector`` is accepted and ignored. Keypoints are not
+supported.
 """
 
 from __future__ import annotations
@@ -37,6 +38,12 @@ import yaml
 def sub_dir(sim_dir: Path, source_idx: int) -> Path:
     """``util.get_sub_dir`` (big-wave/util.py:92-97)."""
     return Path(sim_dir) / f"{source_idx:08}"
+
+
+def detector_x_vector(detector_size: float, pixel_size_x: float) -> np.ndarray:
+    """``util.detector_x_vector`` (big-wave/util.py:78-82)."""
+    n = detector_size // pixel_size_x
+    return (np.arange(n) - n // 2) * pixel_size_x
 
 
 def _load(path: Path):
@@ -101,8 +108,6 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, dtype: Opt
                           history_dz: Optional[float] = None) -> np.ndarray:
     """Run source ``source_idx`` of ``sim_dir`` and write its detected.npy
     (big-wave/multisim.py:50-150). Returns the detector array."""
-    if history_dz is not None:
-        raise ValueError("history recording is not supported by the fused engine")
     from .engine import Simulation
 
     sim_dir = Path(sim_dir)
@@ -116,10 +121,18 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, dtype: Opt
             field = field.astype(want)  # the reference converts with a warning (config.py:155-160)
     sim = Simulation(c, grids=c["grids"], dtype=dt, cutoff_angles=c["cutoff_angles"])
     try:
+        sim.set_history(history_dz)
         sim.reset()
         sim.run_source(energy=c["energy"], db_table=c["db"], source=c["source"], field=field)
         det = sim.detected()
         out_dir = sub_dir(sim_dir, source_idx)
+        if history_dz:
+            h, z = sim.history()
+            sp = c["sim_params"]
+            np.save(out_dir / "history.npy", h)
+            np.save(out_dir / "history_z.npy", z)
+            np.save(out_dir / "history_x.npy",
+                    detector_x_vector(sp["detector_size"], sp["detector_pixel_size_x"]))
         np.save(out_dir / "detected.npy", det)
         if c["save_final_u_vectors"]:
             if det.shape[0] != 1:

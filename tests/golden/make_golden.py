@@ -274,6 +274,20 @@ def _cases():
     c6["sim_params"]["chunk_size"] = 5000
     cases.append(c6)
 
+    # 7./8. history recording (big-wave/history.py:43-135): a point source
+    #    through the three-grating interferometer (analytic source history,
+    #    gaps re-propagated from their start, grating sub-steps), and the
+    #    sample case (pushes before every sample row).
+    c7 = json.loads(json.dumps(cases[2]))
+    c7["name"] = "hist_point_tl"
+    c7["history_dz"] = 0.02
+    cases.append(c7)
+    c8 = json.loads(json.dumps({k: v for k, v in cases[4].items() if k != "grid"}))
+    c8["name"] = "hist_sample"
+    c8["grid"] = grid
+    c8["history_dz"] = 0.013
+    cases.append(c8)
+
     return cases
 
 
@@ -320,11 +334,18 @@ def _run_case(case, mods, tmp: Path):
     U = vector.NumpyVector(np.zeros(N, np.complex128))
     sub = tmp / "sub"
     sub.mkdir(exist_ok=True)
+    hist = None
+    if case.get("history_dz"):
+        import history as bw_history
+        hist = (bw_history.History(), float(case["history_dz"]))
     det = wavesim.run_simulation(
         params, s, elements, list(case["cutoff_angles"]), u, U, db_table,
-        sub, sub, bool(case.get("save_u", False)),
+        sub, sub, bool(case.get("save_u", False)), history=hist,
     )
     out = {"detected": np.array(det)}
+    if hist is not None:
+        out["history"] = hist[0].get_history()
+        out["history_z"] = np.array(hist[0].get_z(), dtype=np.float64)
     if case.get("save_u"):
         us = sorted(sub.glob("u_*.npy"))
         # phase step 0 only, to keep the fixture small

@@ -77,3 +77,15 @@ def test_fft2_golden():
 def test_energy_conversion():
     # big-wave/test.py:201-207
     assert abs(bw.wavelength_from_energy(46000) - 26.95e-12) < 0.01e-12
+
+
+@pytest.mark.parametrize("name", ["hist_point_tl", "hist_sample"])
+def test_oracle_history_matches_reference(name):
+    """History recording (big-wave/history.py) against the reference's own
+    History of the same run."""
+    case, grids, d = load_case(name)
+    det, h, z = bw.run_simulation(case, grids, history_dz=case["history_dz"])
+    assert np.array_equal(z, d["history_z"])
+    assert h.shape == d["history"].shape
+    assert rel_l2(h, d["history"]) < 1e-13
+    assert rel_l2(det, d["detected"]) < 1e-13

@@ -99,9 +99,13 @@ def test_rejects_bad_dtype_and_sources(tmp_path):
 def test_cli_reports_errors_without_traceback(tmp_path, capsys):
     assert simdir.main([str(tmp_path / "missing"), "-s", "0"]) == 1
     assert "error:" in capsys.readouterr().err
-    _write_snapshot_dir(tmp_path)
-    assert simdir.main([str(tmp_path), "-s", "0", "--history_dz", "0.01"]) == 1
-    assert "history" in capsys.readouterr().err
+
+
+def test_detector_x_vector_matches_reference_formula():
+    # util.detector_x_vector (big-wave/util.py:78-82)
+    x = simdir.detector_x_vector(2.5e-05, 1.0e-06)
+    n = 2.5e-05 // 1.0e-06
+    assert np.array_equal(x, (np.arange(n) - n // 2) * 1.0e-06)
 
 
 # ------------------------------------------------------------------ on the GPU
@@ -150,3 +154,20 @@ def test_sample_dir_vector_source(tmp_path, dtype, tol):
     assert det.shape == d["detected"].shape
     assert rel_l2(det, d["detected"]) < tol
     assert np.array_equal(np.load(tmp_path / "00000000" / "detected.npy"), det)
+
+
+@gpu
+def test_cli_history(tmp_path):
+    _need_cuda()
+    from oracle import bigwave_np as bw
+
+    _write_snapshot_dir(tmp_path)
+    assert simdir.main([str(tmp_path), "-s", "0", "--history_dz", "0.05"]) == 0
+    sub = tmp_path / "00000000"
+    h, z, x = (np.load(sub / f) for f in ("history.npy", "history_z.npy", "history_x.npy"))
+    case, _ = load_snapshot_case()
+    det, h_ref, z_ref = bw.run_simulation(case, history_dz=0.05)
+    assert np.array_equal(z, z_ref)
+    assert h.shape == h_ref.shape
+    assert rel_l2(h, h_ref) < 1e-10
+    assert x.shape == (h.shape[0],)
