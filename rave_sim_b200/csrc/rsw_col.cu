@@ -2,25 +2,25 @@
 #include "rsw_passes.cuh"
 
 namespace rsw {
-#define RSW_COL_CASE(R, L, C) \
-    case L: return e == 32 ? col_impl<R, L, C, 32>(a, s) : col_impl<R, L, C, 16>(a, s);
-#define RSW_COL_CASE16(R, L, C) \
-    case L: return col_impl<R, L, C, 16>(a, s);
+#define RSW_COL_CASE(R, L) \
+    case L: return e == 32 ? col_impl<R, L, 4, 32>(a, s) : col_impl<R, L, col_c(L), 16>(a, s);
+#define RSW_COL_CASE16(R, L) \
+    case L: return col_impl<R, L, col_c(L), 16>(a, s);
 
 
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) {
     if (dbl) {
         switch (a.log_n1) {
-            RSW_COL_CASE16(double, 4, 4) RSW_COL_CASE16(double, 5, 4) RSW_COL_CASE16(double, 6, 4)
-            RSW_COL_CASE16(double, 7, 4) RSW_COL_CASE16(double, 8, 4) RSW_COL_CASE(double, 9, 4)
-            RSW_COL_CASE(double, 10, 4) RSW_COL_CASE(double, 11, 4)
+            RSW_COL_CASE16(double, 4) RSW_COL_CASE16(double, 5) RSW_COL_CASE16(double, 6)
+            RSW_COL_CASE16(double, 7) RSW_COL_CASE16(double, 8) RSW_COL_CASE(double, 9)
+            RSW_COL_CASE(double, 10) RSW_COL_CASE(double, 11)
         default: return cudaErrorInvalidValue;
         }
     }
     switch (a.log_n1) {
-        RSW_COL_CASE16(float, 4, 4) RSW_COL_CASE16(float, 5, 4) RSW_COL_CASE16(float, 6, 4)
-        RSW_COL_CASE16(float, 7, 4) RSW_COL_CASE16(float, 8, 4) RSW_COL_CASE(float, 9, 4)
-        RSW_COL_CASE(float, 10, 4) RSW_COL_CASE(float, 11, 4) RSW_COL_CASE(float, 12, 4)
+        RSW_COL_CASE16(float, 4) RSW_COL_CASE16(float, 5) RSW_COL_CASE16(float, 6)
+        RSW_COL_CASE16(float, 7) RSW_COL_CASE16(float, 8) RSW_COL_CASE(float, 9)
+        RSW_COL_CASE(float, 10) RSW_COL_CASE(float, 11) RSW_COL_CASE(float, 12)
     default: return cudaErrorInvalidValue;
     }
 }

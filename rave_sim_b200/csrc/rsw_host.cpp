@@ -404,15 +404,16 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
         if (lg > row_max + 2 * col_max)
             return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the three-level limit 2^%d for this dtype", lg,
                         row_max + 2 * col_max);
-        // outer columns of at least 2^7 (the pass with the transmission and
-        // the twiddle tables); the middle level runs plain FFTs
+        // long outer columns (the pass with the transmission and the factor
+        // tables, which amortise over the column length); the middle level
+        // runs plain FFTs of what is left, at least 2^4
         const int rest = lg - row_max;
         *lr = row_max;
-        *l1 = std::max(7, (rest + 1) / 2);
+        *l1 = std::min(std::min(col_max, 11), rest - 4);
         *lb = rest - *l1;
-        if (*lb < 4) {
-            *lb = 4;
-            *l1 = rest - 4;
+        if (*lb > col_max) {
+            *lb = col_max;
+            *l1 = rest - col_max;
         }
         return RSW_OK;
     }

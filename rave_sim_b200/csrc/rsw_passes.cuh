@@ -236,6 +236,12 @@ __device__ __forceinline__ int k2_bound(int64_t x, int log_n1, int l) {
     return c < 0 ? 0 : (c > l ? l : int(c));
 }
 
+// layout of the column kernel's per-column four-step factors
+constexpr int COL_LO = 66;  // 64 low factors with a pad after each 32
+__device__ __forceinline__ int col_lo(int k1) { return (k1 & 63) + ((k1 & 63) >> 5); }
+template <int L> constexpr int col_nvx() { return COL_LO + ((L >> 6) > 0 ? (L >> 6) : 1); }
+template <int L> constexpr int col_nvp() { return col_nvx<L>() + ((2 - col_nvx<L>()) % 16 + 16) % 16; }
+
 // ------------------------------------------------------------------ passes
 // Persistent kernels: one CTA per SM loops over rows (column tiles); block
 // twiddles are copied to shared memory once per CTA, four-step twiddles of a
@@ -397,8 +403,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     using B = Block<Real, LOG_L1, C, E>;
     using Cx = typename B::Cx;
     constexpr int L = B::L;
-    constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
-    constexpr int NVP = NV | 1;  // odd per-column stride: the C columns' factors fall in different banks
+    // Per-column four-step factors: 64 low ones at e + (e >> 5) (a pad after
+    // every 32: the lanes of one wavefront read low factors 32 apart), the
+    // high ones from COL_LO, per-column stride = 2 mod 16 (the C columns of a
+    // wavefront fall in different banks).
+    constexpr int NVX = col_nvx<L>();
+    constexpr int NVP = col_nvp<L>();
     extern __shared__ __align__(16) unsigned char smraw[];
     const int t = threadIdx.x;
     const int c = t % C;
@@ -427,9 +437,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         const int64_t base = batch << (LOG_L1 + log_n2);
         if (flags & (PF_TW | PF_TWI)) {
             // W_M^{n2 k1} = A[k1 & 63] * B[k1 >> 6] for each of the C columns
-            for (int idx = t; idx < C * NV; idx += B::NT) {
-                const int cc = idx / NV, e = idx % NV;
-                const int64_t m = ((e < 64 ? int64_t(e) : int64_t(e - 64) << 6) * (col0 + cc)) & nmask;
+            for (int idx = t; idx < C * NVX; idx += B::NT) {
+                const int cc = idx / NVX, e = idx % NVX;
+                if (e == 32 || e == COL_LO - 1) continue;  // pads
+                // slot e < 32 holds factor e, slots 33..64 factors 32..63 (col_lo)
+                const int64_t f = e < COL_LO ? int64_t(e < 32 ? e : e - 1) : int64_t(e - COL_LO) << 6;
+                const int64_t m = (f * (col0 + cc)) & nmask;
                 vec[cc * NVP + e] = cvt(w4(a, m), Cx{});
             }
         }
@@ -447,7 +460,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int k1 = B::last_freq(tp, r);
-                    v[r] = cscale(cmulc(cmulc(v[r], vc[k1 & 63]), vc[64 + (k1 >> 6)]), s);
+                    v[r] = cscale(cmulc(cmulc(v[r], vc[col_lo(k1)]), vc[COL_LO + (k1 >> 6)]), s);
                 }
             }
             B::inverse(sm, tp, v, tw);
@@ -468,7 +481,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int k1 = B::last_freq(tp, r);
-                    v[r] = cmul(v[r], cmul(vc[k1 & 63], vc[64 + (k1 >> 6)]));
+                    v[r] = cmul(v[r], cmul(vc[col_lo(k1)], vc[COL_LO + (k1 >> 6)]));
                 }
             }
 #pragma unroll
@@ -527,15 +540,27 @@ template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(con
     return cudaGetLastError();
 }
 
+// Columns per CTA of the column kernel (16 samples per thread): enough for
+// 256-thread CTAs and 512-byte row segments on short columns, 4 (64-byte
+// segments) from 2^10 up; capped so that the factor tables still fit.
+constexpr int col_c(int log_l) {
+    return log_l <= 5 ? 64 : log_l <= 7 ? 32 : log_l == 8 ? 16 : log_l == 9 ? 8 : 4;
+}
+
 template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
     auto k = col_pass_kernel<Real, LG, C, E>;
-    const size_t smem = B::SMEM + 2 * size_t(C) * (n_vec<B::L>() | 1) * sizeof(typename B::Cx);
-    static cudaError_t attr = prep(k, smem);
+    // the per-column factor tables only when the pass applies a four-step twiddle
+    const size_t plain = B::SMEM;
+    const size_t tab = B::SMEM + 2 * size_t(C) * col_nvp<B::L>() * sizeof(typename B::Cx);
+    static cudaError_t attr = prep(k, tab);
     if (attr != cudaSuccess) return attr;
-    static int64_t cap = resident_ctas(k, B::NT, smem);
+    static int64_t cap_tab = resident_ctas(k, B::NT, tab);
+    static int64_t cap_plain = resident_ctas(k, B::NT, plain);
+    const bool tables = a.flags & (PF_TW | PF_TWI);
+    const int64_t cap = tables ? cap_tab : cap_plain;
     const int64_t tiles = (a.n >> LG) / C;
-    k<<<dim3(unsigned(tiles < cap ? tiles : cap)), dim3(B::NT), smem, s>>>(a);
+    k<<<dim3(unsigned(tiles < cap ? tiles : cap)), dim3(B::NT), tables ? tab : plain, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }
