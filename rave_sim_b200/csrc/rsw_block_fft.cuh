@@ -25,7 +25,7 @@
 // leaves natural order, so no register permutation is ever needed.
 //
 // Twiddles W_{RS}^{jq} of stage s live in shared memory, loaded once per CTA:
-// a direct table [(q-1)*S + j] for strides S <= 128, otherwise two factors
+// a direct table [(q-1)*S + j] for strides S <= 128 (512 for complex64), otherwise two factors
 // W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64 entries per q.
 // Shared memory holds the C sequences with one pad element per 16 (phys(p))
 // and a per-sequence pitch chosen so that the accesses of one wavefront hit
@@ -124,17 +124,18 @@ template <int R, int DIR, typename C> __device__ __forceinline__ void net_dit(C 
 
 // Radix structure of a block of length 2^LOG_L with E_ elements per thread
 // (the stage structure and twiddle layout do not depend on E_).
-template <int LOG_L, int E_ = 16> struct Radix {
+template <int LOG_L, int E_ = 16, int MAX_LS = 7> struct Radix {
     static_assert(LOG_L >= 4, "blocks hold at least 16 elements");
-    static_assert(E_ == 16 || E_ == 32, "16 or 32 elements per thread");
+    static_assert(E_ == 8 || E_ == 16 || E_ == 32, "8, 16 or 32 elements per thread");
     static constexpr int L = 1 << LOG_L;
     static constexpr int E = E_;
+    static constexpr int RB = digit_bits(E_);  // radix 2^RB stages
     static constexpr int T = L / E;  // threads per sequence
-    static constexpr int NS = stage_count(LOG_L);
-    __host__ __device__ static constexpr int lr(int s) { return stage_lr(LOG_L, s); }
-    __host__ __device__ static constexpr int ls(int s) { return stage_ls(LOG_L, s); }
-    __host__ __device__ static constexpr bool direct(int s) { return stage_direct(LOG_L, s); }
-    __host__ __device__ static constexpr int twoff(int s) { return stage_tw_offset(LOG_L, s); }
+    static constexpr int NS = stage_count(LOG_L, RB);
+    __host__ __device__ static constexpr int lr(int s) { return stage_lr(LOG_L, s, RB); }
+    __host__ __device__ static constexpr int ls(int s) { return stage_ls(LOG_L, s, RB); }
+    __host__ __device__ static constexpr bool direct(int s) { return stage_direct(LOG_L, s, MAX_LS, RB); }
+    __host__ __device__ static constexpr int twoff(int s) { return stage_tw_offset(LOG_L, s, MAX_LS, RB); }
     static constexpr int TW = twoff(NS - 1) > 0 ? twoff(NS - 1) : 1;
     // butterflies per thread in stage s
     __host__ __device__ static constexpr int M(int s) { return E >> lr(s); }
@@ -148,8 +149,9 @@ template <int LOG_L, int E_ = 16> struct Radix {
     __host__ __device__ static constexpr int group(int s) { return s == 0 ? T : (1 << (lr(s) + ls(s))) / E; }
 };
 
-template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG_L, E_> {
-    using Rx = Radix<LOG_L, E_>;
+template <typename Real, int LOG_L, int C, int E_ = 16>
+struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
+    using Rx = Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))>;
     using Cx = typename CxT<Real>::T;
     using Rx::E;
     using Rx::L;
@@ -301,8 +303,8 @@ template <typename Real, int LOG_L, int C, int E_ = 16> struct Block : Radix<LOG
     // a per-thread part and a compile-time part with disjoint bits:
     // last_freq(tp, r) == freq_base(tp) | freq_off(r).
     static constexpr int last_off(int r) { return (r / RL) * RL + brev_bits(r % RL, Rx::lr(NS - 1)); }
-    static constexpr int freq_off(int r) { return digitrev_c(last_off(r), LOG_L); }
-    __device__ static __forceinline__ int freq_base(int tp) { return digitrev_c(tp * E, LOG_L); }
+    static constexpr int freq_off(int r) { return digitrev_c(last_off(r), LOG_L, Rx::RB); }
+    __device__ static __forceinline__ int freq_base(int tp) { return digitrev_c(tp * E, LOG_L, Rx::RB); }
     __device__ static __forceinline__ int last_freq(int tp, int r) { return freq_base(tp) | freq_off(r); }
 
     // copy the block's twiddle tables (global, host-built layout) into shared memory

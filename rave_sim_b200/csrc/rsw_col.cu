@@ -4,6 +4,9 @@
 namespace rsw {
 #define RSW_COL_CASE(R, L) \
     case L: return e == 32 ? col_impl<R, L, 4, 32>(a, s) : col_impl<R, L, col_c(L), 16>(a, s);
+#define RSW_COL_CASE8(R, L) \
+    case L: return e == 8 ? col_impl<R, L, 4, 8>(a, s) \
+                          : e == 32 ? col_impl<R, L, 4, 32>(a, s) : col_impl<R, L, col_c(L), 16>(a, s);
 #define RSW_COL_CASE16(R, L) \
     case L: return col_impl<R, L, col_c(L), 16>(a, s);
 
@@ -13,14 +16,14 @@ cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) 
         switch (a.log_n1) {
             RSW_COL_CASE16(double, 4) RSW_COL_CASE16(double, 5) RSW_COL_CASE16(double, 6)
             RSW_COL_CASE16(double, 7) RSW_COL_CASE16(double, 8) RSW_COL_CASE(double, 9)
-            RSW_COL_CASE(double, 10) RSW_COL_CASE(double, 11)
+            RSW_COL_CASE8(double, 10) RSW_COL_CASE8(double, 11)
         default: return cudaErrorInvalidValue;
         }
     }
     switch (a.log_n1) {
         RSW_COL_CASE16(float, 4) RSW_COL_CASE16(float, 5) RSW_COL_CASE16(float, 6)
         RSW_COL_CASE16(float, 7) RSW_COL_CASE16(float, 8) RSW_COL_CASE(float, 9)
-        RSW_COL_CASE(float, 10) RSW_COL_CASE(float, 11) RSW_COL_CASE(float, 12)
+        RSW_COL_CASE8(float, 10) RSW_COL_CASE8(float, 11) RSW_COL_CASE(float, 12)
     default: return cudaErrorInvalidValue;
     }
 }
@@ -28,6 +31,9 @@ cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) 
 
 #define RSW_CH_CASE(R, L) \
     case L: return e == 32 ? chirp_impl<R, L, 32>(out, hi, lo, s) : chirp_impl<R, L, 16>(out, hi, lo, s);
+#define RSW_CH_CASE8(R, L) \
+    case L: return e == 8 ? chirp_impl<R, L, 8>(out, hi, lo, s) \
+                          : e == 32 ? chirp_impl<R, L, 32>(out, hi, lo, s) : chirp_impl<R, L, 16>(out, hi, lo, s);
 #define RSW_CH_CASE16(R, L) \
     case L: return chirp_impl<R, L, 16>(out, hi, lo, s);
 
@@ -35,15 +41,15 @@ cudaError_t launch_chirp_table(void *out, int log_n2, double hi, double lo, bool
     if (dbl) {
         switch (log_n2) {
             RSW_CH_CASE16(double, 4) RSW_CH_CASE16(double, 5) RSW_CH_CASE16(double, 6) RSW_CH_CASE16(double, 7)
-            RSW_CH_CASE16(double, 8) RSW_CH_CASE(double, 9) RSW_CH_CASE(double, 10) RSW_CH_CASE(double, 11)
-            RSW_CH_CASE(double, 12) RSW_CH_CASE(double, 13)
+            RSW_CH_CASE16(double, 8) RSW_CH_CASE(double, 9) RSW_CH_CASE(double, 10) RSW_CH_CASE8(double, 11)
+            RSW_CH_CASE8(double, 12) RSW_CH_CASE8(double, 13)
         default: return cudaErrorInvalidValue;
         }
     }
     switch (log_n2) {
         RSW_CH_CASE16(float, 4) RSW_CH_CASE16(float, 5) RSW_CH_CASE16(float, 6) RSW_CH_CASE16(float, 7)
-        RSW_CH_CASE16(float, 8) RSW_CH_CASE(float, 9) RSW_CH_CASE(float, 10) RSW_CH_CASE(float, 11)
-        RSW_CH_CASE(float, 12) RSW_CH_CASE(float, 13) RSW_CH_CASE(float, 14)
+        RSW_CH_CASE16(float, 8) RSW_CH_CASE(float, 9) RSW_CH_CASE(float, 10) RSW_CH_CASE8(float, 11)
+        RSW_CH_CASE8(float, 12) RSW_CH_CASE8(float, 13) RSW_CH_CASE(float, 14)
     default: return cudaErrorInvalidValue;
     }
 }

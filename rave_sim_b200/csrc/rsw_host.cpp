@@ -28,10 +28,10 @@
 namespace rsw {
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
-cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
-                                   bool dbl, cudaStream_t s);
-cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
-                                   bool dbl, cudaStream_t s);
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
+                                   cudaStream_t s);
+cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
+                                   cudaStream_t s);
 cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cudaStream_t s);
 cudaError_t launch_retrieval(const double *data, int64_t n_pix, const RetrievalArgs &r, double *dabs, double *dphase,
                              double *dvis, double *chi2, cudaStream_t s);
@@ -328,13 +328,14 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
 // Block twiddle tables of a block of length 2^log_l in the shared-memory
 // layout of the block FFT (rsw_stages.h): stages in order, entry k of stage s
 // is W_{RS}^m with (m, RS) from stage_tw_entry.
-template <typename T> static std::vector<T> block_twiddles(int log_l) {
+template <typename T> static std::vector<T> block_twiddles(int log_l, int rb) {
     std::vector<T> v;
     if (log_l >= 4) {
-        for (int s = 0; s < stage_count(log_l) - 1; ++s) {
-            for (int64_t k = 0; k < stage_tw_entries(log_l, s); ++k) {
+        const int max_ls = direct_max_ls(int(2 * sizeof(T)));
+        for (int s = 0; s < stage_count(log_l, rb) - 1; ++s) {
+            for (int64_t k = 0; k < stage_tw_entries(log_l, s, max_ls, rb); ++k) {
                 int64_t m, mod;
-                stage_tw_entry(log_l, s, k, &m, &mod);
+                stage_tw_entry(log_l, s, max_ls, rb, k, &m, &mod);
                 push_c(v, twiddle(m, mod));
             }
         }
@@ -357,13 +358,13 @@ static rsw_status four_step_tables(int log_m, DevBuf &lo_buf, DevBuf &hi_buf, in
 }
 
 template <typename T> static rsw_status plan_tables(rsw_plan_s *p) {
-    CHECK(p->tw_row.upload(block_twiddles<T>(p->log_nr)));
+    CHECK(p->tw_row.upload(block_twiddles<T>(p->log_nr, digit_bits(p->row_e))));
     if (p->log_n1 > 0) {
-        CHECK(p->tw_col.upload(block_twiddles<T>(p->log_n1)));
+        CHECK(p->tw_col.upload(block_twiddles<T>(p->log_n1, digit_bits(p->col_e))));
         CHECK(four_step_tables(p->log_n, p->tw4_lo, p->tw4_hi, &p->tw4_shift));
     }
     if (p->three()) {
-        CHECK(p->tw_mid.upload(block_twiddles<T>(p->log_nb)));
+        CHECK(p->tw_mid.upload(block_twiddles<T>(p->log_nb, digit_bits(p->mid_e))));
         CHECK(four_step_tables(p->log_n2, p->tw4b_lo, p->tw4b_hi, &p->tw4b_shift));
     }
     return RSW_OK;
@@ -447,9 +448,12 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
     return RSW_OK;
 }
 
-// Kernel variant per block size: elements per thread (16 or 32). 32 halves the
-// threads of a CTA and lifts the register cap of the large blocks.
-// RSW_ROW_E / RSW_COL_E override the choice (tuning sweeps).
+// Kernel variant per block size: elements per thread. Columns of 2^11 (and
+// 2^10 in two-level plans) take 8 per thread (radix-8 stages, 1024-thread
+// CTAs at 64 registers: twice the warps per SM of the 16-per-thread kernels,
+// measured 9 % faster for complex64 and 2.5 % for complex128); everything
+// else 16.
+// RSW_ROW_E / RSW_COL_E (8, 16 or 32) override the choice (tuning sweeps).
 static int env_int(const char *name, int dflt) {
     const char *v = std::getenv(name);
     return v && *v ? std::atoi(v) : dflt;
@@ -457,11 +461,15 @@ static int env_int(const char *name, int dflt) {
 static void choose_tuning(rsw_plan_s *p) {
     auto pick = [](int log_l, int dflt) { return log_l >= 9 ? dflt : 16; };
     p->row_e = pick(p->log_nr, 16);
-    p->col_e = pick(p->log_n1, 16);
+    // (2^10 outer columns of three-level plans measured faster with 16)
+    p->col_e = (p->log_n1 == 11 || (p->log_n1 == 10 && p->log_nb == 0)) ? 8 : pick(p->log_n1, 16);
     p->mid_e = pick(p->log_nb, 16);
     const int re = env_int("RSW_ROW_E", 0), ce = env_int("RSW_COL_E", 0);
     if ((re == 16 || re == 32) && p->log_nr >= 9) p->row_e = re;
     if ((ce == 16 || ce == 32) && p->log_n1 >= 9) p->col_e = ce;
+    // 8 samples per thread: multi-level rows of 2^11..2^13, columns of 2^10..2^11
+    if (re == 8 && p->log_n1 > 0 && p->log_nr >= 11 && p->log_nr <= 13) p->row_e = 8;
+    if (ce == 8 && p->log_n1 >= 10 && p->log_n1 <= 11) p->col_e = 8;
 }
 
 // Arguments of the outer column pass (and of single-level row passes).
@@ -486,6 +494,8 @@ static PassArgs base_args(const rsw_plan_s *p) {
     a.tw4_shift = p->tw4_shift;
     a.tw_log = p->log_n;
     a.tw_scale = 1.0 / double(p->n);
+    a.rb_n1 = digit_bits(p->col_e);
+    a.rb_nb = digit_bits(p->mid_e);
     a.pr.fac = 1.0 / double(p->n);
     a.tr.kind = TR_NONE;
     return a;
@@ -675,11 +685,15 @@ rsw_status rsw_plan_info(rsw_plan p, int64_t *n, int *dtype, int *log_rows, int 
 
 static rsw_status need_scratch(rsw_plan_s *p) { return p->scratch.alloc(size_t(p->n) * p->elem()); }
 
+static SpecLevels spec_levels(const rsw_plan_s *p) {
+    return SpecLevels{p->log_n1, p->log_nb, p->log_nr, digit_bits(p->col_e), digit_bits(p->mid_e),
+                      digit_bits(p->row_e)};
+}
 static cudaError_t to_natural(const rsw_plan_s *p, const void *spec, void *nat, cudaStream_t s) {
-    return launch_spec_to_natural(spec, nat, p->n, p->log_n1, p->log_nb, p->log_nr, p->dbl(), s);
+    return launch_spec_to_natural(spec, nat, p->n, spec_levels(p), p->dbl(), s);
 }
 static cudaError_t to_spec(const rsw_plan_s *p, const void *nat, void *spec, cudaStream_t s) {
-    return launch_natural_to_spec(nat, spec, p->n, p->log_n1, p->log_nb, p->log_nr, p->dbl(), s);
+    return launch_natural_to_spec(nat, spec, p->n, spec_levels(p), p->dbl(), s);
 }
 
 rsw_status rsw_fft_forward(rsw_plan p, const void *in, void *out, void *stream) {

@@ -84,6 +84,7 @@ struct PassArgs {
     int log_n1;
     int log_n2;
     int log_nb;     // row kernel: middle level (0: none)
+    int rb_n1, rb_nb;  // row kernel: digit widths of the column and middle levels (digitrev of the row)
     int flags;
     const void *tw_row;   // block twiddles of the row level
     const void *tw_col;   // block twiddles of the column level
@@ -94,6 +95,13 @@ struct PassArgs {
     double tw_scale;      // factor of the conjugate twiddles (1/N at the last inverse level)
     TransArgs tr;
     PropArgs pr;
+};
+
+// Level structure of the internal spectrum layout (log2 lengths and digit
+// widths of the column, middle and row levels).
+struct SpecLevels {
+    int log_n1, log_nb, log_nr;
+    int rb_n1, rb_nb, rb_nr;
 };
 
 // Phase-step signal retrieval: the 3 x K pseudo-inverse of [sin phi_k,

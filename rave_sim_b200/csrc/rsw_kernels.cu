@@ -23,25 +23,24 @@ cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) 
 // internal spectrum layout <-> natural frequency order. Frequency
 // k = k1 + N1 (kb + Nb kr) sits at ((p1 Nb + pb) Nr + pr), p = digitpos of
 // each level's index (log_nb = 0 for two-level and single-level plans).
-__device__ __forceinline__ int64_t spec_addr(int64_t k, int log_n1, int log_nb, int log_nr) {
-    const int64_t k1 = k & ((int64_t(1) << log_n1) - 1);
-    const int64_t kb = (k >> log_n1) & ((int64_t(1) << log_nb) - 1);
-    const int64_t kr = k >> (log_n1 + log_nb);
-    return (((digitpos_rt(k1, log_n1) << log_nb) + digitpos_rt(kb, log_nb)) << log_nr) + digitpos_rt(kr, log_nr);
+__device__ __forceinline__ int64_t spec_addr(int64_t k, const SpecLevels &v) {
+    const int64_t k1 = k & ((int64_t(1) << v.log_n1) - 1);
+    const int64_t kb = (k >> v.log_n1) & ((int64_t(1) << v.log_nb) - 1);
+    const int64_t kr = k >> (v.log_n1 + v.log_nb);
+    return (((digitpos_rt(k1, v.log_n1, v.rb_n1) << v.log_nb) + digitpos_rt(kb, v.log_nb, v.rb_nb)) << v.log_nr) +
+           digitpos_rt(kr, v.log_nr, v.rb_nr);
 }
 template <typename Cx>
-__global__ void spec_to_natural_kernel(const Cx *__restrict__ in, Cx *__restrict__ out, int64_t n,
-                                       int log_n1, int log_nb, int log_nr) {
+__global__ void spec_to_natural_kernel(const Cx *__restrict__ in, Cx *__restrict__ out, int64_t n, SpecLevels v) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride)
-        out[k] = in[spec_addr(k, log_n1, log_nb, log_nr)];
+        out[k] = in[spec_addr(k, v)];
 }
 template <typename Cx>
-__global__ void natural_to_spec_kernel(const Cx *__restrict__ in, Cx *__restrict__ out, int64_t n,
-                                       int log_n1, int log_nb, int log_nr) {
+__global__ void natural_to_spec_kernel(const Cx *__restrict__ in, Cx *__restrict__ out, int64_t n, SpecLevels v) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride)
-        out[spec_addr(k, log_n1, log_nb, log_nr)] = in[k];
+        out[spec_addr(k, v)] = in[k];
 }
 
 template <typename Cx>
@@ -124,26 +123,22 @@ static unsigned grid_for(int64_t n, int threads) {
     return unsigned(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
-cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
-                                   bool dbl, cudaStream_t s) {
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
+                                   cudaStream_t s) {
     ++g_launches;
     if (dbl)
-        spec_to_natural_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((const double2 *)in, (double2 *)out, n,
-                                                                          log_n1, log_nb, log_nr);
+        spec_to_natural_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((const double2 *)in, (double2 *)out, n, v);
     else
-        spec_to_natural_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((const float2 *)in, (float2 *)out, n,
-                                                                        log_n1, log_nb, log_nr);
+        spec_to_natural_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((const float2 *)in, (float2 *)out, n, v);
     return cudaGetLastError();
 }
-cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
-                                   bool dbl, cudaStream_t s) {
+cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
+                                   cudaStream_t s) {
     ++g_launches;
     if (dbl)
-        natural_to_spec_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((const double2 *)in, (double2 *)out, n,
-                                                                          log_n1, log_nb, log_nr);
+        natural_to_spec_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((const double2 *)in, (double2 *)out, n, v);
     else
-        natural_to_spec_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((const float2 *)in, (float2 *)out, n,
-                                                                        log_n1, log_nb, log_nr);
+        natural_to_spec_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((const float2 *)in, (float2 *)out, n, v);
     return cudaGetLastError();
 }
 cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cudaStream_t s) {

@@ -36,8 +36,8 @@ namespace rsw {
 rsw_status set_error(rsw_status st, const char *msg);  // message for rsw_last_error()
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
-cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, int log_n1, int log_nb, int log_nr,
-                                   bool dbl, cudaStream_t s);
+cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
+                                   cudaStream_t s);
 }  // namespace rsw
 
 using namespace rsw;
@@ -46,7 +46,7 @@ namespace {
 
 constexpr int64_t MAX_N = RSW_NOALLOC_MAX_N;
 constexpr size_t SPEC_BYTES = size_t(MAX_N) * 16;  // intermediate spectrum, complex128 worst case
-constexpr size_t BLOCK_TW_ENTRIES = 8192;           // per level, >= Radix<13 or 14>::TW
+constexpr size_t BLOCK_TW_ENTRIES = 8192;           // per level, >= the block twiddles of 2^8 (both dtypes)
 constexpr size_t TW4_ENTRIES = 256;                 // 2^ceil(16/2)
 constexpr size_t OFF_TWROW = SPEC_BYTES;
 constexpr size_t OFF_TWCOL = OFF_TWROW + BLOCK_TW_ENTRIES * 16;
@@ -68,11 +68,12 @@ namespace {
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     int off = 0;
+    const int max_ls = direct_max_ls(int(2 * sizeof(T)));
     for (int s = 0; s < stage_count(log_l) - 1; ++s) {
-        const int count = stage_tw_entries(log_l, s);
+        const int count = stage_tw_entries(log_l, s, max_ls);
         for (int k = idx; k < count; k += stride) {
             int64_t m, mod;
-            stage_tw_entry(log_l, s, k, &m, &mod);
+            stage_tw_entry(log_l, s, max_ls, 4, k, &m, &mod);
             double sn, cs;
             sincospi(-2.0 * double(m % mod) / double(mod), &sn, &cs);
             out[2 * (off + k)] = T(cs);
@@ -167,6 +168,8 @@ extern "C" rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int
     a.tw4_hi = scratch + OFF_TW4HI;
     a.tw4_shift = (log_n + 1) / 2;
     a.tw_log = log_n;
+    a.rb_n1 = 4;
+    a.rb_nb = 4;
     a.tw_scale = 1.0 / double(n);
     a.pr.fac = 1.0 / double(n);
     void *spec = scratch;
@@ -183,7 +186,7 @@ extern "C" rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int
     a.out = spec;
     a.flags = PF_FWD;
     if ((e = launch_row_pass(a, dbl, 16, s)) != cudaSuccess) return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
-    if ((e = launch_spec_to_natural(spec, d_out, n, log_n1, 0, log_n2, dbl, s)) != cudaSuccess)
+    if ((e = launch_spec_to_natural(spec, d_out, n, SpecLevels{log_n1, 0, log_n2, 4, 4, 4}, dbl, s)) != cudaSuccess)
         return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
     return RSW_OK;
 }

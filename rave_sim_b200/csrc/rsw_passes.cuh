@@ -229,6 +229,11 @@ __device__ __forceinline__ double2 w4(const PassArgs &a, int64_t m) {
     return cmul(__ldg(lo + (m & mask)), __ldg(hi + (m >> a.tw4_shift)));
 }
 
+// digitrev_rt with the digit width as a compile-time constant (3 or 4)
+__device__ __forceinline__ int64_t digitrev_w(int64_t p, int log_l, int rb) {
+    return rb == 3 ? digitrev_rt(p, log_l, 3) : digitrev_rt(p, log_l, 4);
+}
+
 // ceil(x / 2^log_n1) clamped to [0, l]: the first row frequency k2 with
 // k1 + k2 * 2^log_n1 >= k1 + x
 __device__ __forceinline__ int k2_bound(int64_t x, int log_n1, int l) {
@@ -248,7 +253,9 @@ template <int L> constexpr int col_nvp() { return col_nvx<L>() + ((2 - col_nvx<L
 // row (tile) are factored into 64 + len/64 entries built once per row (tile).
 // CHIRP: transfer function in the factored chirp form (two-level plans), else
 // the per-sample formula (single-level plans).
-template <typename Real, int LOG_L2, int E, bool CHIRP>
+// TWF: the three-level variant with the W_{N2} twiddle before the forward
+// transform (a separate kernel, so that the two-level one carries no code for it)
+template <typename Real, int LOG_L2, int E, bool CHIRP, bool TWF = false>
 __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel(PassArgs a) {
     using B = Block<Real, LOG_L2, 1, E>;
     using Cx = typename B::Cx;
@@ -281,8 +288,8 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         Cx *chp = vec + NV;  // chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
         // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
         // conjugate four-step twiddle of the innermost split uses tw_k
-        const int64_t k1 = digitrev_rt(row >> a.log_nb, a.log_n1);
-        const int64_t kb = digitrev_rt(row & ((int64_t(1) << a.log_nb) - 1), a.log_nb);
+        const int64_t k1 = digitrev_w(row >> a.log_nb, a.log_n1, a.rb_n1);
+        const int64_t kb = digitrev_w(row & ((int64_t(1) << a.log_nb) - 1), a.log_nb, a.rb_nb);
         const int64_t kbase = k1 + (kb << a.log_n1);
         const int64_t tw_k = a.log_nb > 0 ? kb : k1;
         if (CHIRP && a.pr.has_h) {
@@ -319,7 +326,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         if (!(flags & PF_SPEC_IN)) {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[B::first_pos(tp, r)];
-            if (flags & PF_TWF) {
+            if (TWF && (flags & PF_TWF)) {
                 __syncthreads();  // this row's factor table is complete
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
@@ -527,9 +534,9 @@ template <typename K> static int64_t resident_ctas(K kernel, int threads, size_t
 template <int L> constexpr int n_vec() { return 64 + ((L >> 6) > 0 ? (L >> 6) : 1); }
 template <int L> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) : 2); }
 
-template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
+template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
-    auto k = row_pass_kernel<Real, LG, E, CH>;
+    auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
     const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L>()) * sizeof(typename B::Cx);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
@@ -538,6 +545,12 @@ template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(con
     k<<<dim3(unsigned(rows < cap ? rows : cap)), dim3(B::NT), smem, s>>>(a);
     count_launch();
     return cudaGetLastError();
+}
+template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
+    if constexpr (CH) {
+        if (a.flags & PF_TWF) return row_launch<Real, LG, E, true, true>(a, s);
+    }
+    return row_launch<Real, LG, E, CH, false>(a, s);
 }
 
 // Columns per CTA of the column kernel (16 samples per thread): enough for

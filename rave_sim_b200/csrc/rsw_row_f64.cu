@@ -9,6 +9,11 @@ namespace rsw {
                          : row_impl<R, L, 16, false>(a, s);
 #define RSW_ROW_CASE16(R, L) \
     case L: return chirp ? row_impl<R, L, 16, true>(a, s) : row_impl<R, L, 16, false>(a, s);
+// rows with 8 samples per thread (radix-8 stages, twice the threads)
+#define RSW_ROW_CASE8(R, L) \
+    case L: return chirp ? (e == 8 ? row_impl<R, L, 8, true>(a, s) \
+                                   : e == 32 ? row_impl<R, L, 32, true>(a, s) : row_impl<R, L, 16, true>(a, s)) \
+                         : row_impl<R, L, 16, false>(a, s);
 #define RSW_ROW_CASE_S(R, L) \
     case L: return chirp ? cudaErrorInvalidValue : row_impl<R, L, 16, false>(a, s);
 
@@ -17,7 +22,7 @@ cudaError_t launch_row_pass_f64(const PassArgs &a, int e, cudaStream_t s) {
     switch (a.log_n2) {
             RSW_ROW_CASE_S(double, 4) RSW_ROW_CASE_S(double, 5) RSW_ROW_CASE_S(double, 6)
             RSW_ROW_CASE16(double, 7) RSW_ROW_CASE16(double, 8) RSW_ROW_CASE(double, 9)
-            RSW_ROW_CASE(double, 10) RSW_ROW_CASE(double, 11) RSW_ROW_CASE(double, 12) RSW_ROW_CASE(double, 13)
+            RSW_ROW_CASE(double, 10) RSW_ROW_CASE8(double, 11) RSW_ROW_CASE8(double, 12) RSW_ROW_CASE8(double, 13)
         default: return cudaErrorInvalidValue;
         }
 }

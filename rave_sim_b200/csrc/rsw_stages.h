@@ -2,8 +2,9 @@
 // twiddle-table builder and the device table builder of the no-allocation
 // entry point, so that all three agree on one layout.
 //
-// A block of length L = 2^log_l is transformed in NS = ceil(log_l / 4)
-// stages: radix-16 stages first, the remaining radix 2/4/8/16 last. Stage s
+// A block of length L = 2^log_l is transformed in NS = ceil(log_l / rb)
+// stages of digit width rb (radix 2^rb: 16 for kernels with 16 or 32 samples
+// per thread, 8 for 8 samples per thread), the remainder radix last. Stage s
 // has radix R_s = 2^lr(s) and stride S_s = 2^ls(s), with
 // ls(s) = log_l - (lr(0) + ... + lr(s)); the last stage has stride 1.
 // Forward stages are decimation in frequency (large strides first), so the
@@ -11,9 +12,11 @@
 //     f = sum_s digit_s(p) * R_0 * ... * R_{s-1},   digit_s(p) = (p >> ls(s)) mod R_s.
 //
 // Twiddles W_{R S}^{j q} (q = 1..R-1, j < S) of every stage but the last are
-// stored per stage: direct [(q-1) S + j] for S <= 2^RSW_DIRECT_MAX_LS,
-// otherwise factored into W^{(j & 63) q} at [(q-1) 64 + (j & 63)] and
-// W^{64 (j >> 6) q} at [(R-1) 64 + (q-1) (S/64) + (j >> 6)].
+// stored per stage: direct [(q-1) S + j] for S <= 2^max_ls, otherwise
+// factored into W^{(j & 63) q} at [(q-1) 64 + (j & 63)] and
+// W^{64 (j >> 6) q} at [(R-1) 64 + (q-1) (S/64) + (j >> 6)]. max_ls depends
+// on the element size (direct_max_ls): complex64 tables stay direct up to
+// strides of 512 (61 KB), complex128 ones up to 128 (30 KB).
 #pragma once
 
 #include <stdint.h>
@@ -26,32 +29,37 @@
 
 namespace rsw {
 
-constexpr int RSW_DIRECT_MAX_LS = 7;
+RSW_HD constexpr int direct_max_ls(int elem_bytes) { return elem_bytes <= 8 ? 9 : 7; }
 
-RSW_HD constexpr int stage_count(int log_l) { return log_l <= 0 ? 0 : (log_l + 3) / 4; }
-RSW_HD constexpr int stage_lr(int log_l, int s) {
-    return s < stage_count(log_l) - 1 ? 4 : log_l - 4 * (stage_count(log_l) - 1);
+// digit width of the kernels with e samples per thread
+RSW_HD constexpr int digit_bits(int e) { return e == 8 ? 3 : 4; }
+
+RSW_HD constexpr int stage_count(int log_l, int rb = 4) { return log_l <= 0 ? 0 : (log_l + rb - 1) / rb; }
+RSW_HD constexpr int stage_lr(int log_l, int s, int rb = 4) {
+    return s < stage_count(log_l, rb) - 1 ? rb : log_l - rb * (stage_count(log_l, rb) - 1);
 }
-RSW_HD constexpr int stage_ls(int log_l, int s) { return s < stage_count(log_l) - 1 ? log_l - 4 * (s + 1) : 0; }
-RSW_HD constexpr bool stage_direct(int log_l, int s) { return stage_ls(log_l, s) <= RSW_DIRECT_MAX_LS; }
+RSW_HD constexpr int stage_ls(int log_l, int s, int rb = 4) {
+    return s < stage_count(log_l, rb) - 1 ? log_l - rb * (s + 1) : 0;
+}
+RSW_HD constexpr bool stage_direct(int log_l, int s, int max_ls, int rb = 4) { return stage_ls(log_l, s, rb) <= max_ls; }
 // twiddle entries of stage s (none for the last stage)
-RSW_HD constexpr int stage_tw_entries(int log_l, int s) {
-    return s >= stage_count(log_l) - 1 ? 0
-           : stage_direct(log_l, s)
-               ? ((1 << stage_lr(log_l, s)) - 1) << stage_ls(log_l, s)
-               : ((1 << stage_lr(log_l, s)) - 1) * (64 + (1 << (stage_ls(log_l, s) - 6)));
+RSW_HD constexpr int stage_tw_entries(int log_l, int s, int max_ls, int rb = 4) {
+    return s >= stage_count(log_l, rb) - 1 ? 0
+           : stage_direct(log_l, s, max_ls, rb)
+               ? ((1 << stage_lr(log_l, s, rb)) - 1) << stage_ls(log_l, s, rb)
+               : ((1 << stage_lr(log_l, s, rb)) - 1) * (64 + (1 << (stage_ls(log_l, s, rb) - 6)));
 }
-RSW_HD constexpr int stage_tw_offset(int log_l, int s) {
+RSW_HD constexpr int stage_tw_offset(int log_l, int s, int max_ls, int rb = 4) {
     int o = 0;
-    for (int t = 0; t < s; ++t) o += stage_tw_entries(log_l, t);
+    for (int t = 0; t < s; ++t) o += stage_tw_entries(log_l, t, max_ls, rb);
     return o;
 }
 
 // exponent m and modulus R*S of table entry k of stage s: the entry is W_{RS}^m
-RSW_HD inline void stage_tw_entry(int log_l, int s, int64_t k, int64_t *m, int64_t *mod) {
-    const int64_t R = int64_t(1) << stage_lr(log_l, s), S = int64_t(1) << stage_ls(log_l, s);
+RSW_HD inline void stage_tw_entry(int log_l, int s, int max_ls, int rb, int64_t k, int64_t *m, int64_t *mod) {
+    const int64_t R = int64_t(1) << stage_lr(log_l, s, rb), S = int64_t(1) << stage_ls(log_l, s, rb);
     *mod = R * S;
-    if (stage_direct(log_l, s)) {
+    if (stage_direct(log_l, s, max_ls, rb)) {
         *m = (k / S + 1) * (k % S);
     } else if (k < (R - 1) * 64) {
         *m = (k / 64 + 1) * (k % 64);
@@ -64,34 +72,34 @@ RSW_HD inline void stage_tw_entry(int log_l, int s, int64_t k, int64_t *m, int64
 // Frequency index held at block position p after the forward stages. The map
 // is a permutation of the bits of p, so positions with disjoint bits map to
 // frequencies with disjoint bits: digitrev(a | b) == digitrev(a) | digitrev(b).
-RSW_HD constexpr int digitrev_c(int p, int log_l) {
+RSW_HD constexpr int digitrev_c(int p, int log_l, int rb = 4) {
     int f = 0, sh = 0;
-    for (int s = 0; s < stage_count(log_l); ++s) {
-        const int lr = stage_lr(log_l, s);
-        f |= ((p >> stage_ls(log_l, s)) & ((1 << lr) - 1)) << sh;
+    for (int s = 0; s < stage_count(log_l, rb); ++s) {
+        const int lr = stage_lr(log_l, s, rb);
+        f |= ((p >> stage_ls(log_l, s, rb)) & ((1 << lr) - 1)) << sh;
         sh += lr;
     }
     return f;
 }
-RSW_HD inline int64_t digitrev_rt(int64_t p, int log_l) {
-    const int ns = stage_count(log_l);
+RSW_HD inline int64_t digitrev_rt(int64_t p, int log_l, int rb = 4) {
+    const int ns = stage_count(log_l, rb);
     int64_t f = 0;
     int sh = 0;
     for (int s = 0; s < ns; ++s) {
-        const int lr = stage_lr(log_l, s);
-        f |= ((p >> stage_ls(log_l, s)) & ((int64_t(1) << lr) - 1)) << sh;
+        const int lr = stage_lr(log_l, s, rb);
+        f |= ((p >> stage_ls(log_l, s, rb)) & ((int64_t(1) << lr) - 1)) << sh;
         sh += lr;
     }
     return f;
 }
 // Inverse of digitrev_rt: frequency index -> block position.
-RSW_HD inline int64_t digitpos_rt(int64_t f, int log_l) {
-    const int ns = stage_count(log_l);
+RSW_HD inline int64_t digitpos_rt(int64_t f, int log_l, int rb = 4) {
+    const int ns = stage_count(log_l, rb);
     int64_t p = 0;
     int sh = 0;
     for (int s = 0; s < ns; ++s) {
-        const int lr = stage_lr(log_l, s);
-        p |= ((f >> sh) & ((int64_t(1) << lr) - 1)) << stage_ls(log_l, s);
+        const int lr = stage_lr(log_l, s, rb);
+        p |= ((f >> sh) & ((int64_t(1) << lr) - 1)) << stage_ls(log_l, s, rb);
         sh += lr;
     }
     return p;
