@@ -27,9 +27,10 @@
 // Twiddles W_{RS}^{jq} of stage s live in shared memory, loaded once per CTA:
 // a direct table [(q-1)*S + j] for strides S <= 128 (512 for complex64), otherwise two factors
 // W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64 entries per q.
-// Shared memory holds the C sequences with one pad element per 16 (phys(p))
-// and a per-sequence pitch chosen so that the accesses of one wavefront hit
-// distinct banks.
+// Shared memory holds the C sequences with one pad element per E (phys(p):
+// the last stage gives consecutive threads positions E apart, which the pad
+// moves to neighbouring banks) and a per-sequence pitch chosen so that the
+// accesses of one wavefront hit distinct banks.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -159,14 +160,15 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
     using Rx::T;
     static constexpr int NT = T * C;  // threads per CTA
     static constexpr int W = 32 / int(sizeof(Cx) / 4);  // elements per smem wavefront
-    static constexpr int BASE = L + L / 16;
+    static constexpr int LOG_E = ilog2(E_);
+    static constexpr int BASE = L + (L >> LOG_E);
     static constexpr int WANT = (C >= W) ? 1 : W / C;
     static constexpr int PITCH = BASE + (((WANT - BASE) % W) + W) % W;
     static constexpr size_t DATA = size_t(C) * PITCH * sizeof(Cx);
     static constexpr size_t SMEM = DATA + size_t(Rx::TW) * sizeof(Cx);
     static constexpr int RL = 1 << Rx::lr(NS - 1);  // radix of the last stage
 
-    __device__ static __forceinline__ int phys(int p) { return p + (p >> 4); }
+    __device__ static __forceinline__ int phys(int p) { return p + (p >> LOG_E); }
 
     template <int s> __device__ static __forceinline__ int pos(int tp, int i, int q) {
         constexpr int LRS = Rx::lr(s), LSS = Rx::ls(s);
