@@ -31,6 +31,11 @@ namespace rsw {
 // ---------------------------------------------------------------- counters
 __device__ __forceinline__ double rint_d(double x) { return rint(x); }
 
+// L2 prefetch of [p, p + bytes): p 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Range reduction of a phase to [-pi, pi] (Cody & Waite 1980, three-part
 // constant; 2pi = P1 + P2 + P3 with P1, P2 of 29 significant bits so that
 // k*P1 and k*P2 are exact for |k| < 2^24), then sincos of the remainder.
@@ -241,11 +246,20 @@ __device__ __forceinline__ int k2_bound(int64_t x, int log_n1, int l) {
     return c < 0 ? 0 : (c > l ? l : int(c));
 }
 
-// layout of the column kernel's per-column four-step factors
-constexpr int COL_LO = 66;  // 64 low factors with a pad after each 32
-__device__ __forceinline__ int col_lo(int k1) { return (k1 & 63) + ((k1 & 63) >> 5); }
-template <int L> constexpr int col_nvx() { return COL_LO + ((L >> 6) > 0 ? (L >> 6) : 1); }
-template <int L> constexpr int col_nvp() { return col_nvx<L>() + ((2 - col_nvx<L>()) % 16 + 16) % 16; }
+// Layout of the column kernel's four-step factors (one copy per tile
+// parity): per column, the thread-part factors X (2^LX, stride XP) and Y
+// (2^LY, stride YP) in FP64, then the E register parts (stride E + 1) in the
+// field's precision. T = threads per column.
+template <int T> struct ColTab {
+    static constexpr int LOG_T = ilog2(T);
+    static constexpr int LX = (LOG_T + 1) / 2, LY = LOG_T - LX;
+    static constexpr int XP = (1 << LX) + 2, YP = (1 << LY) + 1;
+    template <int C, int E, int CX> static constexpr size_t parity_bytes() {
+        return (size_t(C) * (XP + YP) * 16 + size_t(C) * (E + 1) * CX + 15) / 16 * 16;
+    }
+    // bytes after the block's data and twiddles (16 of them for alignment)
+    template <int C, int E, int CX> static constexpr size_t bytes() { return 16 + 2 * parity_bytes<C, E, CX>(); }
+};
 
 // ------------------------------------------------------------------ passes
 // Persistent kernels: one CTA per SM loops over rows (column tiles); block
@@ -265,6 +279,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
     Cx *sm = reinterpret_cast<Cx *>(smraw);
     Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
     constexpr int NQ = (L >> 6) > 1 ? (L >> 6) : 2;  // k2s >> 6 spans [-NQ/2, NQ/2)
+    constexpr int NCH = 64 + NQ + E;  // chirp factors per row: P, Q and the per-register R
     const int tp = threadIdx.x;
     const int flags = a.flags;
     const int64_t rows = a.n >> LOG_L2;
@@ -284,8 +299,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
     for (int64_t row = blockIdx.x; row < rows; row += gridDim.x, parity ^= 1) {
         // per-row tables, double-buffered by row parity: the next row fills
         // the other copy while slower warps still read this one
-        Cx *vec = tw + B::TW + parity * (NV + 64 + NQ);  // four-step factors: [0,64) low, [64, NV) high
-        Cx *chp = vec + NV;  // chirp factors: [0,64) P[k2s & 63], [64, 64+NQ) Q[(k2s >> 6) + NQ/2]
+        Cx *vec = tw + B::TW + parity * (NV + NCH);  // four-step factors: [0,64) low, [64, NV) high
+        // chirp factors: [0,64) P[a], [64, 64+NQ) Q[b + NQ/2], [64+NQ, NCH) R[r]
+        Cx *chp = vec + NV;
         // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
         // conjugate four-step twiddle of the innermost split uses tw_k
         const int64_t k1 = digitrev_w(row >> a.log_nb, a.log_n1, a.rb_n1);
@@ -294,17 +310,25 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         const int64_t tw_k = a.log_nb > 0 ? kb : k1;
         if (CHIRP && a.pr.has_h) {
             // phase of the row: G kbase^2 + g1 k2s with g1 = 2 M G kbase (turns),
-            // M = 2^log_m; P[a] = A exp(2 pi i (G kbase^2 + g1 a)), Q[b] = exp(2 pi i 64 g1 b)
+            // M = 2^log_m; P[a] = A exp(2 pi i (G kbase^2 + g1 a)), Q[b] = exp(2 pi i 64 g1 b).
+            // k2s = fbase + s_r splits into the thread's part (P[fbase & 63] Q[fbase >> 6],
+            // taken once per row) and the register's part R[r] = exp(2 pi i g1 s_r),
+            // s_r = freq_off(r) - L if the top frequency bit is set (all lanes read
+            // the same R[r])
             const double m = double(int64_t(1) << log_m);
             const double gk = frac_dd(a.pr.g_hi, a.pr.g_lo, double(kbase * kbase));
             const double g1h = 2.0 * m * a.pr.g_hi, g1l = 2.0 * m * a.pr.g_lo;
-            for (int idx = tp; idx < 64 + NQ; idx += B::NT) {
+            for (int idx = tp; idx < NCH; idx += B::NT) {
                 double2 w;
                 if (idx < 64) {
                     w = cmul(a.pr.A, cis_turns(gk + frac_dd(g1h, g1l, double(kbase * idx))));
-                } else {
+                } else if (idx < 64 + NQ) {
                     const int64_t b = int64_t(idx - 64) - NQ / 2;
                     w = cis_turns(frac_dd(g1h, g1l, double(kbase * 64 * b)));
+                } else {
+                    const int fo = B::freq_off(idx - 64 - NQ);
+                    const int64_t sr = (fo & (L >> 1)) ? int64_t(fo) - L : int64_t(fo);
+                    w = cis_turns(frac_dd(g1h, g1l, double(kbase * sr)));
                 }
                 chp[idx] = cvt(w, Cx{});
             }
@@ -322,6 +346,16 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
         const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + (row << LOG_L2);
         Cx *__restrict__ gout = static_cast<Cx *>(a.out) + (row << LOG_L2);
+        {
+            // this CTA's next row into L2 while this one is transformed
+            constexpr uint32_t chunk = uint32_t(L * sizeof(Cx) / 32);
+            if constexpr (chunk >= 16 && chunk % 16 == 0) {
+                if (!(flags & PF_ONES) && row + gridDim.x < rows && tp < 32)
+                    prefetch_l2_bulk(reinterpret_cast<const unsigned char *>(gin + (int64_t(gridDim.x) << LOG_L2)) +
+                                         tp * chunk,
+                                     chunk);
+            }
+        }
         Cx v[E];
         if (!(flags & PF_SPEC_IN)) {
 #pragma unroll
@@ -354,14 +388,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
             }
             const unsigned cut_span = unsigned(k2hi - k2lo);
             if (a.pr.has_h) {
-                // H = P[k2s & 63] * Q[k2s >> 6] * h3[r][tp]; k2 >= L/2 (k2s = k2 - L)
-                // is decided by the compile-time part of the frequency
+                // H = P[fbase & 63] * Q[fbase >> 6] * R[r] * h3[r][tp]; k2 >= L/2
+                // (k2s = k2 - L) is decided by the compile-time part of the
+                // frequency, so 0 <= fbase < L/2
                 const Cx *h3 = static_cast<const Cx *>(a.pr.h3);
+                const Cx tb = cmul(chp[fbase & 63], chp[64 + (fbase >> 6) + NQ / 2]);
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int k2 = fbase | B::freq_off(r);
-                    const int k2s = (B::freq_off(r) & (L >> 1)) ? k2 - L : k2;
-                    const Cx h = cmul(cmul(chp[k2s & 63], chp[64 + (k2s >> 6) + NQ / 2]), __ldg(h3 + r * B::T + tp));
+                    const Cx h = cmul(cmul(tb, chp[64 + NQ + r]), __ldg(h3 + r * B::T + tp));
                     v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : cmul(v[r], h);
                 }
             } else {
@@ -410,12 +445,17 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     using B = Block<Real, LOG_L1, C, E>;
     using Cx = typename B::Cx;
     constexpr int L = B::L;
-    // Per-column four-step factors: 64 low ones at e + (e >> 5) (a pad after
-    // every 32: the lanes of one wavefront read low factors 32 apart), the
-    // high ones from COL_LO, per-column stride = 2 mod 16 (the C columns of a
-    // wavefront fall in different banks).
-    constexpr int NVX = col_nvx<L>();
-    constexpr int NVP = col_nvp<L>();
+    // Four-step factor W_M^(n2 k1) of column n2 = col0 + c at the frequency
+    // k1 = freq_base(tp) | freq_off(r) held by register r: the thread's part
+    // W^(n2 freq_base(tp)) times the register's part W^(n2 freq_off(r)) (E
+    // per column, read by every lane of the column). freq_base is a bit
+    // permutation, so the thread part is X[tp & (2^LX - 1)] * Y[tp >> LX] with
+    // X[i] = W^(n2 freq_base(i)), Y[j] = W^(n2 freq_base(j 2^LX)), multiplied
+    // in FP64. The strides put the C columns of a wavefront in different banks.
+    using CT = ColTab<B::T>;
+    constexpr int LX = CT::LX, NX = 1 << LX, NXY = NX + (1 << CT::LY);
+    constexpr int XP = CT::XP, YP = CT::YP, EP = E + 1;
+    constexpr size_t PAR = CT::template parity_bytes<C, E, int(sizeof(Cx))>();
     extern __shared__ __align__(16) unsigned char smraw[];
     const int t = threadIdx.x;
     const int c = t % C;
@@ -434,23 +474,28 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     // a barrier; every other flow ends its tile with one.
     const bool paired = (flags & PF_FWD) && (flags & PF_INV);
 
+    unsigned char *tab0 = smraw + (B::SMEM + 15) / 16 * 16;
+
     int parity = 0;
     for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, parity ^= 1) {
-        // per-column four-step factors (NV per column), double-buffered by tile parity
-        Cx *vec = tw + B::TW + parity * (C * NVP);
+        // factor tables, double-buffered by tile parity
+        double2 *tx = reinterpret_cast<double2 *>(tab0 + parity * PAR);
+        double2 *ty = tx + C * XP;
+        Cx *vec = reinterpret_cast<Cx *>(ty + C * YP);
         const int64_t batch = tile >> log_tb;
         const int64_t col0 = (tile & ((int64_t(1) << log_tb) - 1)) * C;  // column within the batch
         const int64_t col = col0 + c;
         const int64_t base = batch << (LOG_L1 + log_n2);
         if (flags & (PF_TW | PF_TWI)) {
-            // W_M^{n2 k1} = A[k1 & 63] * B[k1 >> 6] for each of the C columns
-            for (int idx = t; idx < C * NVX; idx += B::NT) {
-                const int cc = idx / NVX, e = idx % NVX;
-                if (e == 32 || e == COL_LO - 1) continue;  // pads
-                // slot e < 32 holds factor e, slots 33..64 factors 32..63 (col_lo)
-                const int64_t f = e < COL_LO ? int64_t(e < 32 ? e : e - 1) : int64_t(e - COL_LO) << 6;
-                const int64_t m = (f * (col0 + cc)) & nmask;
-                vec[cc * NVP + e] = cvt(w4(a, m), Cx{});
+            for (int idx = t; idx < C * (NXY + E); idx += B::NT) {
+                const int cc = idx / (NXY + E), e = idx % (NXY + E);
+                const int64_t n2 = col0 + cc;
+                if (e < NX)
+                    tx[cc * XP + e] = w4(a, (int64_t(B::freq_base(e)) * n2) & nmask);
+                else if (e < NXY)
+                    ty[cc * YP + (e - NX)] = w4(a, (int64_t(B::freq_base((e - NX) << LX)) * n2) & nmask);
+                else
+                    vec[cc * EP + (e - NXY)] = cvt(w4(a, (int64_t(B::freq_off(e - NXY)) * n2) & nmask), Cx{});
             }
         }
         if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
@@ -462,13 +507,11 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
             for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
             if (flags & PF_TWI) {
                 __syncthreads();  // this tile's factor table is complete
-                const Cx *vc = vec + c * NVP;
+                const Cx *vc = vec + c * EP;
+                const Cx w = cvt(cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]), Cx{});
                 const Real s = Real(a.tw_scale);  // a power of two: exact
 #pragma unroll
-                for (int r = 0; r < E; ++r) {
-                    const int k1 = B::last_freq(tp, r);
-                    v[r] = cscale(cmulc(cmulc(v[r], vc[col_lo(k1)]), vc[COL_LO + (k1 >> 6)]), s);
-                }
+                for (int r = 0; r < E; ++r) v[r] = cscale(cmulc(v[r], cmul(w, vc[r])), s);
             }
             B::inverse(sm, tp, v, tw);
         } else {
@@ -484,12 +527,10 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
-                const Cx *vc = vec + c * NVP;
+                const Cx *vc = vec + c * EP;
+                const Cx w = cvt(cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]), Cx{});
 #pragma unroll
-                for (int r = 0; r < E; ++r) {
-                    const int k1 = B::last_freq(tp, r);
-                    v[r] = cmul(v[r], cmul(vc[col_lo(k1)], vc[COL_LO + (k1 >> 6)]));
-                }
+                for (int r = 0; r < E; ++r) v[r] = cmul(v[r], cmul(w, vc[r]));
             }
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[int64_t(B::last_pos(tp, r)) << log_n2] = v[r];
@@ -532,12 +573,12 @@ template <typename K> static int64_t resident_ctas(K kernel, int threads, size_t
 }
 
 template <int L> constexpr int n_vec() { return 64 + ((L >> 6) > 0 ? (L >> 6) : 1); }
-template <int L> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) : 2); }
+template <int L, int E> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) : 2) + E; }
 
 template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
     auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
-    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L>()) * sizeof(typename B::Cx);
+    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * sizeof(typename B::Cx);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
@@ -565,7 +606,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
     auto k = col_pass_kernel<Real, LG, C, E>;
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
-    const size_t tab = B::SMEM + 2 * size_t(C) * col_nvp<B::L>() * sizeof(typename B::Cx);
+    const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, int(sizeof(typename B::Cx))>();
     static cudaError_t attr = prep(k, tab);
     if (attr != cudaSuccess) return attr;
     static int64_t cap_tab = resident_ctas(k, B::NT, tab);
