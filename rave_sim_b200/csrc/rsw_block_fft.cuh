@@ -212,6 +212,12 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
         }
     }
 
+    // Factored twiddles in FP64 come as the running product W^(jq) =
+    // W^(j(q-1)) W^j: one table lookup per butterfly instead of R - 1, with
+    // as many complex products as the two-factor lookups (error below
+    // R ulp). complex64 keeps the lookups.
+    template <int s> static constexpr bool running() { return !Rx::direct(s) && sizeof(Real) == 8; }
+
     // forward stage s: natural in -> radix-R DFT -> bit-reversed out, twiddled
     template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Cx *tw) {
         constexpr int R = 1 << Rx::lr(s);
@@ -221,10 +227,21 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
             net_dif<R, -1>(v + i * R);
             if constexpr (s < NS - 1) {
                 const int j = Rx::beta(s, tp, i) & ((1 << LSS) - 1);
+                if constexpr (running<s>()) {
+                    const Cx w1 = twid<s>(tw, j, 1);
+                    Cx w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    Cx &x = v[reg<s, true>(i, q)];
-                    x = cmul(x, twid<s>(tw, j, q));
+                    for (int q = 1; q < R; ++q) {
+                        Cx &x = v[reg<s, true>(i, q)];
+                        x = cmul(x, w);
+                        if (q < R - 1) w = cmul(w, w1);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 1; q < R; ++q) {
+                        Cx &x = v[reg<s, true>(i, q)];
+                        x = cmul(x, twid<s>(tw, j, q));
+                    }
                 }
             }
         }
@@ -237,10 +254,21 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
         for (int i = 0; i < E / R; ++i) {
             if constexpr (s < NS - 1) {
                 const int j = Rx::beta(s, tp, i) & ((1 << LSS) - 1);
+                if constexpr (running<s>()) {
+                    const Cx w1 = twid<s>(tw, j, 1);
+                    Cx w = w1;
 #pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    Cx &x = v[reg<s, true>(i, q)];
-                    x = cmulc(x, twid<s>(tw, j, q));
+                    for (int q = 1; q < R; ++q) {
+                        Cx &x = v[reg<s, true>(i, q)];
+                        x = cmulc(x, w);
+                        if (q < R - 1) w = cmul(w, w1);
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 1; q < R; ++q) {
+                        Cx &x = v[reg<s, true>(i, q)];
+                        x = cmulc(x, twid<s>(tw, j, q));
+                    }
                 }
             }
             net_dit<R, +1>(v + i * R);
@@ -253,17 +281,19 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
     // synchronises with __syncwarp, larger groups with a named barrier of
     // their own, the whole CTA with __syncthreads. Each position is written
     // in a stage only by the thread that read it in that stage, so one
-    // barrier per exchange orders every access.
+    // barrier per exchange orders every access. With more than 15 groups
+    // (named barriers 1..15) aligned pairs, quadruples, ... of groups share
+    // one barrier.
+    static constexpr int sync_lanes(int g) { return g >= NT || g <= 32 || NT / g <= 15 ? g : sync_lanes(2 * g); }
     template <int s> __device__ static __forceinline__ void exchange_sync() {
-        constexpr int G = Rx::group(s) * C;
+        constexpr int G = sync_lanes(Rx::group(s) * C);
         if constexpr (G >= NT) {
             __syncthreads();
         } else if constexpr (G <= 32) {
             __syncwarp();
-        } else if constexpr (NT / G <= 15) {
-            asm volatile("bar.sync %0, %1;" ::"r"(1 + int(threadIdx.x) / G), "r"(G) : "memory");
         } else {
-            __syncthreads();
+            static_assert(NT / G <= 15, "named barriers 1..15");
+            asm volatile("bar.sync %0, %1;" ::"r"(1 + int(threadIdx.x) / G), "r"(G) : "memory");
         }
     }
 

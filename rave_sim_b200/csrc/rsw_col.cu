@@ -9,6 +9,10 @@ namespace rsw {
                           : e == 32 ? col_impl<R, L, 4, 32>(a, s) : col_impl<R, L, col_c(L), 16>(a, s);
 #define RSW_COL_CASE16(R, L) \
     case L: return col_impl<R, L, col_c(L), 16>(a, s);
+// complex64, 2^10 and 2^11: col_c64 columns per tile with 16 per thread
+#define RSW_COL_CASE64_8(L) \
+    case L: return e == 8 ? col_impl<float, L, 4, 8>(a, s) \
+                          : e == 32 ? col_impl<float, L, 4, 32>(a, s) : col_impl<float, L, col_c64(L), 16>(a, s);
 
 
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) {
@@ -23,7 +27,7 @@ cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) 
     switch (a.log_n1) {
         RSW_COL_CASE16(float, 4) RSW_COL_CASE16(float, 5) RSW_COL_CASE16(float, 6)
         RSW_COL_CASE16(float, 7) RSW_COL_CASE16(float, 8) RSW_COL_CASE(float, 9)
-        RSW_COL_CASE8(float, 10) RSW_COL_CASE8(float, 11) RSW_COL_CASE(float, 12)
+        RSW_COL_CASE64_8(10) RSW_COL_CASE64_8(11) RSW_COL_CASE(float, 12)
     default: return cudaErrorInvalidValue;
     }
 }
