@@ -448,13 +448,15 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
     return RSW_OK;
 }
 
-// Kernel variant per block size: elements per thread. Columns of 2^10 in
-// two-level plans (at most 2^21 samples: too few tiles of 16 columns for 148
-// SMs) and complex128 columns of 2^11 take 8 per thread (radix-8 stages,
-// 1024-thread CTAs at 64 registers: twice the warps per SM of the
-// 16-per-thread kernels). Other complex64 columns of 2^10 and 2^11 keep 16
-// per thread, which leaves room for 16 or 8 columns per CTA (128- or 64-byte
-// row segments). Everything else takes 16.
+// Kernel variant per block size: elements per thread. complex128 columns of
+// 2^8 .. 2^11 take 8 per thread (radix-8 stages, 512- or 1024-thread CTAs:
+// two to four times the warps per SM of the 16-per-thread kernels, which
+// hold up to 252 registers at 256 threads; measured 9-20 % faster), as do
+// complex64 columns of 2^9 (16 per CTA, 6 %) and of 2^10 in two-level plans
+// (at most 2^21 samples: too few tiles of 16 columns for 148 SMs). Other
+// complex64 columns of 2^10 and 2^11 keep 16 per thread, which leaves room
+// for 16 or 8 columns per CTA (128- or 64-byte row segments; 8 per thread
+// with 4 columns measured 26-40 % slower). Everything else takes 16.
 // RSW_ROW_E / RSW_COL_E (8, 16 or 32) override the choice (tuning sweeps).
 static int env_int(const char *name, int dflt) {
     const char *v = std::getenv(name);
@@ -463,15 +465,16 @@ static int env_int(const char *name, int dflt) {
 static void choose_tuning(rsw_plan_s *p) {
     auto pick = [](int log_l, int dflt) { return log_l >= 9 ? dflt : 16; };
     p->row_e = pick(p->log_nr, 16);
-    // (2^10 outer columns of three-level plans measured faster with 16)
-    p->col_e = (p->log_n1 == 11 && p->dtype == RSW_C128) || (p->log_n1 == 10 && p->log_nb == 0) ? 8 : pick(p->log_n1, 16);
+    const bool c128 = p->dtype == RSW_C128;
+    const int l1 = p->log_n1;
+    p->col_e = (c128 && l1 >= 8 && l1 <= 11) || (!c128 && (l1 == 9 || (l1 == 10 && p->log_nb == 0))) ? 8 : pick(l1, 16);
     p->mid_e = pick(p->log_nb, 16);
     const int re = env_int("RSW_ROW_E", 0), ce = env_int("RSW_COL_E", 0);
     if ((re == 16 || re == 32) && p->log_nr >= 9) p->row_e = re;
-    if ((ce == 16 || ce == 32) && p->log_n1 >= 9) p->col_e = ce;
-    // 8 samples per thread: multi-level rows of 2^11..2^13, columns of 2^10..2^11
+    if (ce == 16 || (ce == 32 && p->log_n1 >= 9)) p->col_e = ce;
+    // 8 samples per thread: multi-level rows of 2^11..2^13, columns of 2^8..2^11
     if (re == 8 && p->log_n1 > 0 && p->log_nr >= 11 && p->log_nr <= 13) p->row_e = 8;
-    if (ce == 8 && p->log_n1 >= 10 && p->log_n1 <= 11) p->col_e = 8;
+    if (ce == 8 && p->log_n1 >= 8 && p->log_n1 <= 11) p->col_e = 8;
 }
 
 // Arguments of the outer column pass (and of single-level row passes).
