@@ -96,6 +96,19 @@ rsw_status rsw_fft_inverse(rsw_plan plan, const void *d_in, void *d_out, void *s
 #define RSW_NOALLOC_MAX_N 65536
 rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int64_t n, int dtype, void *stream);
 
+/* Out-of-core FFT of a field held in HOST memory (pinned or pageable), for
+ * fields larger than the device's memory. Replaces big-fourier's fft / ifft
+ * (big-fourier/src/bfft.rs:27-100; Python bfpy.fft_c16 / ifft_c16 / fft_c8 /
+ * ifft_c8, big-fourier/src/lib.rs:65-126, called by big-wave/vector.py:134-146)
+ * with the same four-step split and NumPy convention (inverse scaled by 1/N).
+ * The field streams through three device slabs within device_bytes (at least
+ * 3 * 2^ceil(log2(N)/2) samples); the GPU runs every transform pass.
+ * h_scratch holds N samples of intermediate results; NULL uses h_out.
+ * h_out may equal h_in when a separate scratch is given; the scratch must not
+ * be h_in. N is a power of two >= 256. Synchronises `stream` before returning. */
+rsw_status rsw_fft_host(const void *h_in, void *h_out, void *h_scratch, int64_t n, int dtype, int inverse,
+                        int64_t device_bytes, void *stream);
+
 /* big-wave propagation.propagate (big-wave/propagation.py:100-138) and
  * fast-wave propagate<S> (fast-wave/src/simulation.cpp:34-40): u <- iFFT(H * FFT(u))
  * with H the Fresnel transfer function of distance dz and the big-wave frequency

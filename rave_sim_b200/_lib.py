@@ -106,6 +106,7 @@ SIGNATURES = {
     "rsw_fft_forward": (C.c_int, [_P, _P, _P, _P]),
     "rsw_fft_inverse": (C.c_int, [_P, _P, _P, _P]),
     "rsw_fft_forward_noalloc": (C.c_int, [_P, _P, _I64, C.c_int, _P]),
+    "rsw_fft_host": (C.c_int, [_P, _P, _P, _I64, C.c_int, C.c_int, _I64, _P]),
     "rsw_propagate": (C.c_int, [_P, _P, _P, _D, _D, _D, _D, C.c_int, _P]),
     "rsw_apply_grating_factors": (C.c_int, [_P, _P, _D, _I64, _D, _D, _D, _DP, _DP, _P]),
     "rsw_apply_dba_grating_factors": (C.c_int, [_P, _P, _D, _I64, _D, _D, _D, _D, _D, _DP, _DP, _P]),

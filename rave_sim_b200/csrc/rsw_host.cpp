@@ -36,6 +36,9 @@ cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cuda
 cudaError_t launch_retrieval(const double *data, int64_t n_pix, const RetrievalArgs &r, double *dabs, double *dphase,
                              double *dvis, double *chi2, cudaStream_t s);
 cudaError_t launch_copy(const void *in, void *out, int64_t n, bool dbl, cudaStream_t s);
+cudaError_t launch_transpose(const void *in, void *out, int64_t rows, int64_t cols, bool dbl, cudaStream_t s);
+cudaError_t launch_ooc_twiddle(void *u, int64_t count, int log_len, int64_t row0, int log_n, bool inverse, bool dbl,
+                               cudaStream_t s);
 cudaError_t launch_point_source(void *u, int64_t n, double dx, double w, double z, double x_src, bool dbl,
                                 cudaStream_t s);
 cudaError_t launch_detect(const void *u, const int64_t *bounds, const double *cosv, const double *rv,
@@ -396,6 +399,17 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
             return RSW_OK;
         }
     }
+    // RSW_SPLIT = "l1" forces a two-level split with columns of 2^l1 when
+    // valid, also for lengths that fit one row (tests and tuning sweeps)
+    const char *ov = std::getenv("RSW_SPLIT");
+    if (ov && *ov) {
+        const int oa = std::atoi(ov), ob = lg - oa;
+        if (oa >= 4 && oa <= col_max && ob >= 7 && ob <= row_max) {
+            *l1 = oa;
+            *lr = ob;
+            return RSW_OK;
+        }
+    }
     if (lg <= row_max) {
         *l1 = 0;
         *lr = lg;
@@ -433,15 +447,6 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
     if (b > row_max) {
         a = lg - row_max;
         b = row_max;
-    }
-    // RSW_SPLIT overrides the column level (tuning sweeps) when valid
-    const char *ov = std::getenv("RSW_SPLIT");
-    if (ov && *ov) {
-        const int oa = std::atoi(ov), ob = lg - oa;
-        if (oa >= 4 && oa <= col_max && ob >= 7 && ob <= row_max) {
-            a = oa;
-            b = ob;
-        }
     }
     *l1 = a;
     *lr = b;
@@ -745,6 +750,116 @@ rsw_status rsw_fft_inverse(rsw_plan p, const void *in, void *out, void *stream) 
         a.flags = PF_SPEC_IN | PF_INV | PF_SCALE;
         CHECK(run_row(p, a, s));
     }
+    return RSW_OK;
+}
+
+// ------------------------------------------------------------ out-of-core FFT
+// Natural-order FFTs (inverse: scaled by 1/len) of `count` consecutive
+// transforms of the plan's length, in -> out (out may equal in), with
+// count * len samples of device work space. The passes of rsw_fft_forward /
+// rsw_fft_inverse run over all transforms at once: the kernels index rows,
+// column batches and spectrum positions within each transform.
+static rsw_status fft_batch(rsw_plan_s *p, const void *in, void *out, int64_t count, bool inverse, void *work,
+                            cudaStream_t s) {
+    const int64_t total = count * p->n;
+    PassArgs a = base_args(p);
+    a.n = total;
+    cudaError_t e;
+    if (!inverse) {
+        a.in = in;
+        a.out = work;
+        if (p->log_n1 > 0) {
+            a.flags = PF_FWD | PF_TW;
+            CHECK(run_col(p, a, s));
+            a.in = work;
+            if (p->three()) CHECK(run_mid(p, a, true, s));
+        }
+        PassArgs r = row_level(p, a);
+        r.flags = PF_FWD | row_tw(p, true, false);
+        CHECK(run_row(p, r, s));
+        e = launch_spec_to_natural(work, out, total, spec_levels(p), p->dbl(), s);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+        return RSW_OK;
+    }
+    e = launch_natural_to_spec(in, work, total, spec_levels(p), p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
+    a.in = work;
+    if (p->log_n1 > 0) {
+        PassArgs r = row_level(p, a);
+        r.out = work;
+        r.flags = PF_SPEC_IN | PF_INV | row_tw(p, false, true);
+        CHECK(run_row(p, r, s));
+        a.out = work;
+        if (p->three()) CHECK(run_mid(p, a, false, s));
+        a.out = out;
+        a.flags = col_inv(p);
+        CHECK(run_col(p, a, s));
+    } else {
+        a.out = out;
+        a.flags = PF_SPEC_IN | PF_INV | PF_SCALE;
+        CHECK(run_row(p, a, s));
+    }
+    return RSW_OK;
+}
+
+// The four-step of big-fourier's out-of-core fft (big-fourier/src/bfft.rs:27-100):
+// x as q rows x r columns (q = 2^floor(l/2), r = 2^ceil(l/2), split_sizes,
+// bfft.rs:11-24); column transforms of length q with the twiddle
+// W_N^(j k1), then row transforms of length r, X[k1 + q k2]. The host arrays
+// stream through three device slabs: column slabs arrive by 2-D copies and are
+// transposed on the device; step 1 writes its transforms contiguously to the
+// scratch array (transform j at j q); step 2 gathers q-strided slabs of it and
+// writes the result with q-strided 2-D copies.
+rsw_status rsw_fft_host(const void *h_in, void *h_out, void *h_scratch, int64_t n, int dtype, int inverse,
+                        int64_t device_bytes, void *stream) {
+    if (!h_in || !h_out) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
+    if (n < 256 || (n & (n - 1)) != 0)
+        return fail(RSW_ERR_UNSUPPORTED, "N = %lld: the out-of-core FFT takes powers of two >= 256", (long long)n);
+    void *h_y = h_scratch ? h_scratch : h_out;
+    if (h_y == h_in) return fail(RSW_ERR_INVALID, "the scratch array (or out, without one) must not be the input");
+    int lg = 0;
+    while ((int64_t(1) << lg) < n) ++lg;
+    const int lq = lg / 2, lr = lg - lq;
+    const int64_t q = int64_t(1) << lq, r = int64_t(1) << lr;
+    const size_t el = dtype == RSW_C128 ? 16 : 8;
+    int64_t slab = n;  // samples per device slab (three slabs)
+    while (slab > r && int64_t(3) * slab * int64_t(el) > device_bytes) slab >>= 1;
+    if (int64_t(3) * slab * int64_t(el) > device_bytes)
+        return fail(RSW_ERR_INVALID, "device_bytes = %lld: at least 3 * 2^%d samples (%lld bytes) are needed",
+                    (long long)device_bytes, lr, (long long)(3 * r * int64_t(el)));
+    rsw_plan pq = nullptr, pr = nullptr;
+    CHECK(rsw_plan_create(&pq, q, dtype));
+    std::unique_ptr<rsw_plan_s, rsw_status (*)(rsw_plan)> gq(pq, rsw_plan_destroy);
+    CHECK(rsw_plan_create(&pr, r, dtype));
+    std::unique_ptr<rsw_plan_s, rsw_status (*)(rsw_plan)> gr(pr, rsw_plan_destroy);
+    DevBuf A, B, W;
+    CHECK(A.alloc(size_t(slab) * el));
+    CHECK(B.alloc(size_t(slab) * el));
+    CHECK(W.alloc(size_t(slab) * el));
+    const bool dbl = dtype == RSW_C128, inv = inverse != 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    const char *in_b = static_cast<const char *>(h_in);
+    char *y_b = static_cast<char *>(h_y), *out_b = static_cast<char *>(h_out);
+    // step 1: columns j0 .. j0 + c of x (q x r)
+    const int64_t c = std::min(r, slab / q);
+    for (int64_t j0 = 0; j0 < r; j0 += c) {
+        CU(cudaMemcpy2DAsync(A.p, c * el, in_b + j0 * el, r * el, c * el, q, cudaMemcpyHostToDevice, s));
+        CU(launch_transpose(A.p, B.p, q, c, dbl, s));
+        CHECK(fft_batch(pq, B.p, B.p, c, inv, W.p, s));
+        CU(launch_ooc_twiddle(B.p, c, lq, j0, lg, inv, dbl, s));
+        CU(cudaMemcpyAsync(y_b + j0 * q * el, B.p, size_t(c * q) * el, cudaMemcpyDeviceToHost, s));
+    }
+    // step 2: frequencies k0 .. k0 + t of the r transforms (r x q in the scratch array)
+    const int64_t t = std::min(q, slab / r);
+    for (int64_t k0 = 0; k0 < q; k0 += t) {
+        CU(cudaMemcpy2DAsync(A.p, t * el, y_b + k0 * el, q * el, t * el, r, cudaMemcpyHostToDevice, s));
+        CU(launch_transpose(A.p, B.p, r, t, dbl, s));
+        CHECK(fft_batch(pr, B.p, B.p, t, inv, W.p, s));
+        CU(launch_transpose(B.p, A.p, t, r, dbl, s));
+        CU(cudaMemcpy2DAsync(out_b + k0 * el, q * el, A.p, t * el, t * el, r, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
     return RSW_OK;
 }
 

@@ -23,12 +23,17 @@ cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) 
 // internal spectrum layout <-> natural frequency order. Frequency
 // k = k1 + N1 (kb + Nb kr) sits at ((p1 Nb + pb) Nr + pr), p = digitpos of
 // each level's index (log_nb = 0 for two-level and single-level plans).
+// Position in the spectrum layout of natural frequency k; indices at and
+// above one transform's length address consecutive transforms (batches).
 __device__ __forceinline__ int64_t spec_addr(int64_t k, const SpecLevels &v) {
+    const int log_len = v.log_n1 + v.log_nb + v.log_nr;
+    const int64_t seq = k >> log_len << log_len;
     const int64_t k1 = k & ((int64_t(1) << v.log_n1) - 1);
     const int64_t kb = (k >> v.log_n1) & ((int64_t(1) << v.log_nb) - 1);
-    const int64_t kr = k >> (v.log_n1 + v.log_nb);
-    return (((digitpos_rt(k1, v.log_n1, v.rb_n1) << v.log_nb) + digitpos_rt(kb, v.log_nb, v.rb_nb)) << v.log_nr) +
-           digitpos_rt(kr, v.log_nr, v.rb_nr);
+    const int64_t kr = (k >> (v.log_n1 + v.log_nb)) & ((int64_t(1) << v.log_nr) - 1);
+    return seq + ((((digitpos_rt(k1, v.log_n1, v.rb_n1) << v.log_nb) + digitpos_rt(kb, v.log_nb, v.rb_nb))
+                   << v.log_nr) +
+                  digitpos_rt(kr, v.log_nr, v.rb_nr));
 }
 template <typename Cx>
 __global__ void spec_to_natural_kernel(const Cx *__restrict__ in, Cx *__restrict__ out, int64_t n, SpecLevels v) {
@@ -117,6 +122,47 @@ __global__ void zero_kernel(double *__restrict__ p, int64_t n) {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = 0.0;
 }
 
+// out (cols x rows) = transpose of in (rows x cols), row-major, through
+// 32 x 32 tiles in shared memory (padded rows: conflict-free columns)
+template <typename Cx>
+__global__ void __launch_bounds__(256) transpose_kernel(const Cx *__restrict__ in, Cx *__restrict__ out,
+                                                        int64_t rows, int64_t cols) {
+    __shared__ Cx tile[32][33];
+    const int64_t tx = (cols + 31) / 32, ty = (rows + 31) / 32;
+    for (int64_t t = blockIdx.x; t < tx * ty; t += gridDim.x) {
+        const int64_t r0 = (t / tx) * 32, c0 = (t % tx) * 32;
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const int64_t r = r0 + i, c = c0 + threadIdx.x;
+            if (r < rows && c < cols) tile[i][threadIdx.x] = in[r * cols + c];
+        }
+        __syncthreads();
+        for (int i = threadIdx.y; i < 32; i += 8) {
+            const int64_t c = c0 + i, r = r0 + threadIdx.x;
+            if (r < rows && c < cols) out[c * rows + r] = tile[threadIdx.x][i];
+        }
+        __syncthreads();
+    }
+}
+
+// Four-step twiddle of the out-of-core FFT: u[j len + k] *= exp(sign 2 pi i
+// ((row0 + j) k mod n) / n) for j < count, k < len (FP64 phase, exact index).
+template <typename Cx>
+__global__ void ooc_twiddle_kernel(Cx *__restrict__ u, int64_t count, int log_len, int64_t row0, int log_n,
+                                   double sign) {
+    const int64_t total = count << log_len;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t nmask = (int64_t(1) << log_n) - 1;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int64_t j = row0 + (i >> log_len), k = i & ((int64_t(1) << log_len) - 1);
+        const double t = ldexp(double((j * k) & nmask), 1 - log_n);  // 2 m / n, exact
+        double sn, cs;
+        sincospi(t, &sn, &cs);
+        const double2 w = make_double2(cs, sign * sn);
+        const double2 v = make_double2(double(u[i].x), double(u[i].y));
+        u[i] = to_c(make_double2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x), Cx{});
+    }
+}
+
 static unsigned grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     const int64_t cap = 148 * 32;
@@ -145,6 +191,23 @@ cudaError_t launch_trans(void *u, int64_t n, const TransArgs &tr, bool dbl, cuda
     ++g_launches;
     if (dbl) trans_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((double2 *)u, n, tr);
     else trans_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((float2 *)u, n, tr);
+    return cudaGetLastError();
+}
+cudaError_t launch_transpose(const void *in, void *out, int64_t rows, int64_t cols, bool dbl, cudaStream_t s) {
+    ++g_launches;
+    const int64_t tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
+    const unsigned g = unsigned(tiles < 148 * 16 ? tiles : 148 * 16);
+    if (dbl) transpose_kernel<double2><<<g, dim3(32, 8), 0, s>>>((const double2 *)in, (double2 *)out, rows, cols);
+    else transpose_kernel<float2><<<g, dim3(32, 8), 0, s>>>((const float2 *)in, (float2 *)out, rows, cols);
+    return cudaGetLastError();
+}
+cudaError_t launch_ooc_twiddle(void *u, int64_t count, int log_len, int64_t row0, int log_n, bool inverse, bool dbl,
+                               cudaStream_t s) {
+    ++g_launches;
+    const int64_t total = count << log_len;
+    const double sign = inverse ? 1.0 : -1.0;
+    if (dbl) ooc_twiddle_kernel<double2><<<grid_for(total, 256), 256, 0, s>>>((double2 *)u, count, log_len, row0, log_n, sign);
+    else ooc_twiddle_kernel<float2><<<grid_for(total, 256), 256, 0, s>>>((float2 *)u, count, log_len, row0, log_n, sign);
     return cudaGetLastError();
 }
 cudaError_t launch_copy(const void *in, void *out, int64_t n, bool dbl, cudaStream_t s) {

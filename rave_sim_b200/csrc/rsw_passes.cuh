@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
         Cx *chp = vec + NV;
         // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
         // conjugate four-step twiddle of the innermost split uses tw_k
-        const int64_t k1 = digitrev_w(row >> a.log_nb, a.log_n1, a.rb_n1);
+        // (rows beyond one transform belong to the next one of a batch)
+        const int64_t k1 = digitrev_w((row >> a.log_nb) & ((int64_t(1) << a.log_n1) - 1), a.log_n1, a.rb_n1);
         const int64_t kb = digitrev_w(row & ((int64_t(1) << a.log_nb) - 1), a.log_nb, a.rb_nb);
         const int64_t kbase = k1 + (kb << a.log_n1);
         const int64_t tw_k = a.log_nb > 0 ? kb : k1;
