@@ -101,8 +101,10 @@ rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int64_t n, int
  * (big-fourier/src/bfft.rs:27-100; Python bfpy.fft_c16 / ifft_c16 / fft_c8 /
  * ifft_c8, big-fourier/src/lib.rs:65-126, called by big-wave/vector.py:134-146)
  * with the same four-step split and NumPy convention (inverse scaled by 1/N).
- * The field streams through three device slabs within device_bytes (at least
- * 3 * 2^ceil(log2(N)/2) samples); the GPU runs every transform pass.
+ * The field streams through two pipelines of three device slabs within
+ * device_bytes (at least 6 * 2^ceil(log2(N)/2) samples), on `stream` and a
+ * second stream, so that uploads, transforms and downloads overlap; the GPU
+ * runs every transform pass.
  * h_scratch holds N samples of intermediate results; NULL uses h_out.
  * h_out may equal h_in when a separate scratch is given; the scratch must not
  * be h_in. N is a power of two >= 256. Synchronises `stream` before returning. */

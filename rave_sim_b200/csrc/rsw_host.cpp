@@ -806,7 +806,7 @@ static rsw_status fft_batch(rsw_plan_s *p, const void *in, void *out, int64_t co
 // x as q rows x r columns (q = 2^floor(l/2), r = 2^ceil(l/2), split_sizes,
 // bfft.rs:11-24); column transforms of length q with the twiddle
 // W_N^(j k1), then row transforms of length r, X[k1 + q k2]. The host arrays
-// stream through three device slabs: column slabs arrive by 2-D copies and are
+// stream through device slabs: column slabs arrive by 2-D copies and are
 // transposed on the device; step 1 writes its transforms contiguously to the
 // scratch array (transform j at j q); step 2 gathers q-strided slabs of it and
 // writes the result with q-strided 2-D copies.
@@ -823,43 +823,66 @@ rsw_status rsw_fft_host(const void *h_in, void *h_out, void *h_scratch, int64_t 
     const int lq = lg / 2, lr = lg - lq;
     const int64_t q = int64_t(1) << lq, r = int64_t(1) << lr;
     const size_t el = dtype == RSW_C128 ? 16 : 8;
-    int64_t slab = n;  // samples per device slab (three slabs)
-    while (slab > r && int64_t(3) * slab * int64_t(el) > device_bytes) slab >>= 1;
-    if (int64_t(3) * slab * int64_t(el) > device_bytes)
-        return fail(RSW_ERR_INVALID, "device_bytes = %lld: at least 3 * 2^%d samples (%lld bytes) are needed",
-                    (long long)device_bytes, lr, (long long)(3 * r * int64_t(el)));
+    // two pipelines of three slabs each, on the caller's stream and a second
+    // one: consecutive slabs alternate, so that one slab's upload, transforms
+    // and download overlap the other's
+    int64_t slab = n;  // samples per device slab
+    while (slab > r && int64_t(6) * slab * int64_t(el) > device_bytes) slab >>= 1;
+    if (int64_t(6) * slab * int64_t(el) > device_bytes)
+        return fail(RSW_ERR_INVALID, "device_bytes = %lld: at least 6 * 2^%d samples (%lld bytes) are needed",
+                    (long long)device_bytes, lr, (long long)(6 * r * int64_t(el)));
     rsw_plan pq = nullptr, pr = nullptr;
     CHECK(rsw_plan_create(&pq, q, dtype));
     std::unique_ptr<rsw_plan_s, rsw_status (*)(rsw_plan)> gq(pq, rsw_plan_destroy);
     CHECK(rsw_plan_create(&pr, r, dtype));
     std::unique_ptr<rsw_plan_s, rsw_status (*)(rsw_plan)> gr(pr, rsw_plan_destroy);
-    DevBuf A, B, W;
-    CHECK(A.alloc(size_t(slab) * el));
-    CHECK(B.alloc(size_t(slab) * el));
-    CHECK(W.alloc(size_t(slab) * el));
+    DevBuf A[2], B[2], W[2];
+    for (int k = 0; k < 2; ++k) {
+        CHECK(A[k].alloc(size_t(slab) * el));
+        CHECK(B[k].alloc(size_t(slab) * el));
+        CHECK(W[k].alloc(size_t(slab) * el));
+    }
     const bool dbl = dtype == RSW_C128, inv = inverse != 0;
-    cudaStream_t s = (cudaStream_t)stream;
+    cudaStream_t st[2] = {(cudaStream_t)stream, nullptr};
+    CU(cudaStreamCreateWithFlags(&st[1], cudaStreamNonBlocking));
+    std::unique_ptr<CUstream_st, cudaError_t (*)(cudaStream_t)> g1(st[1], cudaStreamDestroy);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (auto &e : ev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> ge0(ev[0], cudaEventDestroy), ge1(ev[1], cudaEventDestroy);
+    // both streams start after the caller's prior work and meet between the steps
+    auto join = [&]() -> rsw_status {
+        CU(cudaEventRecord(ev[0], st[0]));
+        CU(cudaEventRecord(ev[1], st[1]));
+        CU(cudaStreamWaitEvent(st[1], ev[0], 0));
+        CU(cudaStreamWaitEvent(st[0], ev[1], 0));
+        return RSW_OK;
+    };
+    CHECK(join());
     const char *in_b = static_cast<const char *>(h_in);
     char *y_b = static_cast<char *>(h_y), *out_b = static_cast<char *>(h_out);
     // step 1: columns j0 .. j0 + c of x (q x r)
     const int64_t c = std::min(r, slab / q);
-    for (int64_t j0 = 0; j0 < r; j0 += c) {
-        CU(cudaMemcpy2DAsync(A.p, c * el, in_b + j0 * el, r * el, c * el, q, cudaMemcpyHostToDevice, s));
-        CU(launch_transpose(A.p, B.p, q, c, dbl, s));
-        CHECK(fft_batch(pq, B.p, B.p, c, inv, W.p, s));
-        CU(launch_ooc_twiddle(B.p, c, lq, j0, lg, inv, dbl, s));
-        CU(cudaMemcpyAsync(y_b + j0 * q * el, B.p, size_t(c * q) * el, cudaMemcpyDeviceToHost, s));
+    for (int64_t j0 = 0, k = 0; j0 < r; j0 += c, k ^= 1) {
+        cudaStream_t s = st[k];
+        CU(cudaMemcpy2DAsync(A[k].p, c * el, in_b + j0 * el, r * el, c * el, q, cudaMemcpyHostToDevice, s));
+        CU(launch_transpose(A[k].p, B[k].p, q, c, dbl, s));
+        CHECK(fft_batch(pq, B[k].p, B[k].p, c, inv, W[k].p, s));
+        CU(launch_ooc_twiddle(B[k].p, c, lq, j0, lg, inv, dbl, s));
+        CU(cudaMemcpyAsync(y_b + j0 * q * el, B[k].p, size_t(c * q) * el, cudaMemcpyDeviceToHost, s));
     }
+    CHECK(join());
     // step 2: frequencies k0 .. k0 + t of the r transforms (r x q in the scratch array)
     const int64_t t = std::min(q, slab / r);
-    for (int64_t k0 = 0; k0 < q; k0 += t) {
-        CU(cudaMemcpy2DAsync(A.p, t * el, y_b + k0 * el, q * el, t * el, r, cudaMemcpyHostToDevice, s));
-        CU(launch_transpose(A.p, B.p, r, t, dbl, s));
-        CHECK(fft_batch(pr, B.p, B.p, t, inv, W.p, s));
-        CU(launch_transpose(B.p, A.p, t, r, dbl, s));
-        CU(cudaMemcpy2DAsync(out_b + k0 * el, q * el, A.p, t * el, t * el, r, cudaMemcpyDeviceToHost, s));
+    for (int64_t k0 = 0, k = 0; k0 < q; k0 += t, k ^= 1) {
+        cudaStream_t s = st[k];
+        CU(cudaMemcpy2DAsync(A[k].p, t * el, y_b + k0 * el, q * el, t * el, r, cudaMemcpyHostToDevice, s));
+        CU(launch_transpose(A[k].p, B[k].p, r, t, dbl, s));
+        CHECK(fft_batch(pr, B[k].p, B[k].p, t, inv, W[k].p, s));
+        CU(launch_transpose(B[k].p, A[k].p, t, r, dbl, s));
+        CU(cudaMemcpy2DAsync(out_b + k0 * el, q * el, A[k].p, t * el, t * el, r, cudaMemcpyDeviceToHost, s));
     }
-    CU(cudaStreamSynchronize(s));
+    CU(cudaStreamSynchronize(st[1]));
+    CU(cudaStreamSynchronize(st[0]));
     return RSW_OK;
 }
 

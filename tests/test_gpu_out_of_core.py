@@ -26,9 +26,9 @@ def cplx(n, seed, dt):
 
 
 def min_device_bytes(n, dt):
-    """three slabs of one row transform: the smallest working set, many slabs"""
+    """six slabs of one row transform: the smallest working set, many slabs"""
     logn = n.bit_length() - 1
-    return 3 * (1 << (logn - logn // 2)) * np.dtype(NP[dt]).itemsize
+    return 6 * (1 << (logn - logn // 2)) * np.dtype(NP[dt]).itemsize
 
 
 @pytest.mark.parametrize("dt", ["c16", "c8"])
