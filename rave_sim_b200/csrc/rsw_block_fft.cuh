@@ -1,8 +1,9 @@
 // Block FFT building blocks for the split-step passes (sm_100a).
 //
 // A "block" transforms C independent sequences of length L = 2^LOG_L held by
-// one CTA. Each thread owns E = 16 (or 32) elements in registers; stages are
-// radix-16, the last one takes the remaining radix 2/4/8/16 (rsw_stages.h).
+// one CTA. Each thread owns E = 8, 16 or 32 elements in registers; stages are
+// radix-8 (E = 8) or radix-16, the last one takes the remaining radix
+// (rsw_stages.h).
 // Forward stages are decimation in frequency: natural order in,
 // digit-reversed order out. Inverse stages are the exact mirror (decimation
 // in time): digit-reversed in, natural out, so a forward/inverse pair needs
@@ -25,8 +26,10 @@
 // leaves natural order, so no register permutation is ever needed.
 //
 // Twiddles W_{RS}^{jq} of stage s live in shared memory, loaded once per CTA:
-// a direct table [(q-1)*S + j] for strides S <= 128 (512 for complex64), otherwise two factors
-// W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64 entries per q.
+// a direct table [(q-1)*S + j] for strides S <= 128 (512 for complex64),
+// otherwise two factors W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64
+// entries per q. FP64 butterflies may take only W^j from the tables and form
+// the other powers as a running product (running()).
 // Shared memory holds the C sequences with one pad element per E (phys(p):
 // the last stage gives consecutive threads positions E apart, which the pad
 // moves to neighbouring banks) and a per-sequence pitch chosen so that the
@@ -212,11 +215,16 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
         }
     }
 
-    // Factored twiddles in FP64 come as the running product W^(jq) =
-    // W^(j(q-1)) W^j: one table lookup per butterfly instead of R - 1, with
-    // as many complex products as the two-factor lookups (error below
-    // R ulp). complex64 keeps the lookups.
-    template <int s> static constexpr bool running() { return !Rx::direct(s) && sizeof(Real) == 8; }
+    // FP64 twiddles as the running product W^(jq) = W^(j(q-1)) W^j (error
+    // below R ulp): one table lookup per butterfly instead of R - 1. For
+    // factored stages this takes as many complex products as the two-factor
+    // lookups. Radix-8 blocks of 2^10 and more (the 1024-thread complex128
+    // column kernels, held back by shared-memory instruction issue) also
+    // trade the direct lookups for R - 2 products: 7 % faster at 2^11.
+    // complex64 keeps the lookups.
+    template <int s> static constexpr bool running() {
+        return sizeof(Real) == 8 && (!Rx::direct(s) || (E == 8 && LOG_L >= 10));
+    }
 
     // forward stage s: natural in -> radix-R DFT -> bit-reversed out, twiddled
     template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Cx *tw) {
