@@ -17,7 +17,12 @@
 // Between steps the buffer holds the "mid" representation (after the row
 // pass); the field itself (natural order) only exists inside the column pass,
 // where the transmission needs it. Small fields (N <= one block) use a single
-// row pass per step.
+// row pass per step. Three-level plans (N = N1 * Nb * Nr) add a middle pass
+// over Nb between the two (the column kernel as a plain batched FFT), with
+// the W_{N2} twiddles in the row pass. The row pass prefetches its next row
+// into L2 while it transforms the current one. Both kernels also run over
+// batches of transforms (n a multiple of one transform's length): rows and
+// column tiles index within their own transform.
 #pragma once
 
 #include <cuda_runtime.h>
