@@ -102,9 +102,11 @@ def run_simulation(params, source, elements, cutoff_angles, u, U, deltabeta_tabl
     """big-wave ``wavesim.run_simulation`` for one source on the fused engine.
     Returns the list of detector arrays (one per phase step); with
     ``save_final_u_vectors`` the final field of the last phase step is left
-    in ``u``."""
-    if history is not None or save_keypoints_path is not None:
-        raise ValueError("history and keypoints are not supported by the fused engine")
+    in ``u``. ``history`` is big-wave's ``(History, dz)`` pair
+    (big-wave/wavesim.py:95, :129-131): the engine records the history and its
+    entries are pushed into the History object in order."""
+    if save_keypoints_path is not None:
+        raise ValueError("keypoints are not supported by the fused engine")
     n = len(u)
     dtype = u.vec.dtype
     config = {
@@ -129,8 +131,14 @@ def run_simulation(params, source, elements, cutoff_angles, u, U, deltabeta_tabl
         else:
             raise ValueError(f"unsupported source {sname}")
         sim.reset()
+        if history is not None:
+            sim.set_history(float(history[1]))
         sim.run_source(energy=1.0, wavelength=float(params.wl), db_table=table, source=src, field=field)
         det = sim.detected()
+        if history is not None:
+            images, zs = sim.history()
+            for e in range(images.shape[1]):
+                history[0].push(images[:, e].copy(), float(zs[e]))
         if save_final_u_vectors:
             u.vec = sim.final_field().cpu().numpy()
         return [det[i] for i in range(det.shape[0])]

@@ -70,8 +70,21 @@ def _mat(m):
     return None if m is None else Material(m[0], m[1])
 
 
-def test_run_simulation_shim_matches_golden():
-    case, grids, d = load_case("tl3g_point_phase")
+class History:
+    """big-wave/history.py:10-40: entries and z pushed in order."""
+
+    def __init__(self):
+        self.entries, self.zs = [], []
+
+    def push(self, downscaled, z):
+        self.entries.append(downscaled)
+        self.zs.append(z)
+
+    def get_history(self):
+        return np.stack(self.entries, axis=-1) if self.entries else np.empty((0, 0))
+
+
+def _shim_inputs(case):
     sp = case["sim_params"]
     params = SimParams(N=sp["N"], dx=sp["dx"], z_detector=sp["z_detector"], detector_size=sp["detector_size"],
                        detector_pixel_size_x=sp["detector_pixel_size_x"],
@@ -85,9 +98,27 @@ def test_run_simulation_shim_matches_golden():
     src = PointSource(x=case["source"]["x"], z=case["source"]["z"])
     u = NumpyVector(np.zeros(sp["N"], np.complex128))
     U = NumpyVector(np.zeros(sp["N"], np.complex128))
+    return params, src, els, table, u, U
+
+
+def test_run_simulation_shim_matches_golden():
+    case, grids, d = load_case("tl3g_point_phase")
+    params, src, els, table, u, U = _shim_inputs(case)
     out = bigwave.run_simulation(params, src, els, case["cutoff_angles"], u, U, table, ".", ".", False)
     assert len(out) == d["detected"].shape[0]
     assert rel_l2(np.array(out), d["detected"]) < 1e-10
+
+
+def test_run_simulation_shim_history():
+    # wavesim.run_simulation(..., history=(History(), dz)) as multisim.py:114-137 calls it
+    case, grids, d = load_case("hist_point_tl")
+    params, src, els, table, u, U = _shim_inputs(case)
+    hist = History()
+    out = bigwave.run_simulation(params, src, els, case["cutoff_angles"], u, U, table, ".", ".", False,
+                                 history=(hist, case["history_dz"]))
+    assert rel_l2(np.array(out), d["detected"]) < 1e-10
+    assert np.array_equal(np.array(hist.zs), d["history_z"])
+    assert rel_l2(hist.get_history(), d["history"]) < 1e-10
 
 
 def test_propagate_and_detect_shims():
