@@ -181,6 +181,53 @@ template <typename Cx> __device__ __forceinline__ Cx apply_trans(const TransArgs
     }
 }
 
+// apply_trans to the E samples of a thread, sample r at index pos(r), with the
+// kind of transmission decided once for all of them. In the column kernel
+// this keeps the compiler from holding every kind's temporaries across the
+// unrolled samples (the 2^11 complex128 kernel at 16 per thread spilled 204
+// bytes per thread before, none after); the row kernel, which transmits only
+// in single-level plans, keeps the per-sample form (its two-level code ran 6 %
+// slower with this one).
+template <int E, typename Cx, typename Pos>
+__device__ __forceinline__ void apply_trans_e(const TransArgs &t, Pos pos, Cx *v) {
+    switch (t.kind) {
+    case TR_SCALAR: {
+        const Cx f = to_c(t.fa, Cx{});
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = cmul(v[r], f);
+        break;
+    }
+    case TR_GRATING:
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const double x = grating_x(t, pos(r));
+            const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0);
+            v[r] = cmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
+        }
+        break;
+    case TR_DBA:
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const double x = grating_x(t, pos(r));
+            const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0) &&
+                           mod_less(x, t.pitch1, t.inv_pitch1, 0.0, t.dc1);
+            v[r] = cmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
+        }
+        break;
+    case TR_SAMPLE:
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            double2 f;
+            if (sample_factor(t, pos(r), &f)) {
+                const double2 ud = make_double2(double(v[r].x), double(v[r].y));
+                v[r] = to_c(cmul(ud, f), Cx{});
+            }
+        }
+        break;
+    default: break;
+    }
+}
+
 // ------------------------------------------------------------ propagator
 // U *= exp(-i2pi dz/wl) * exp(i pi wl dz fx^2), fx = (ks * (1/N)) / dx, zero in
 // the cutoff range (big-wave/propagation.py:74-97, :124-137).
@@ -525,11 +572,8 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
             for (int r = 0; r < E; ++r)
                 v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[int64_t(B::first_pos(tp, r)) << log_n2];
         }
-        if (flags & PF_TRANS) {
-#pragma unroll
-            for (int r = 0; r < E; ++r)
-                v[r] = apply_trans(a.tr, base + (int64_t(B::first_pos(tp, r)) << log_n2) + col, v[r]);
-        }
+        if (flags & PF_TRANS)
+            apply_trans_e<E>(a.tr, [&](int r) { return base + (int64_t(B::first_pos(tp, r)) << log_n2) + col; }, v);
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
