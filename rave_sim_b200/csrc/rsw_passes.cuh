@@ -421,9 +421,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT) row_pass_kernel
                     v[r] = cmulc(cmulc(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
                 }
             }
-            if (flags & PF_TRANS) {
+            // Rows of multi-level plans never transmit (the column pass does).
+            // Leaving the code out of the complex64 kernel frees registers
+            // (5 % faster); the complex128 one ran 2 % slower without it.
+            if constexpr (!(CHIRP && sizeof(Real) == 4)) {
+                if (flags & PF_TRANS) {
 #pragma unroll
-                for (int r = 0; r < E; ++r) v[r] = apply_trans(a.tr, (row << LOG_L2) + B::first_pos(tp, r), v[r]);
+                    for (int r = 0; r < E; ++r)
+                        v[r] = apply_trans(a.tr, (row << LOG_L2) + B::first_pos(tp, r), v[r]);
+                }
             }
             if (flags & PF_FWD) B::forward(sm, tp, v, tw);
         } else {
