@@ -154,8 +154,8 @@ template <int LOG_L, int E_ = 16, int MAX_LS = 7> struct Radix {
 };
 
 template <typename Real, int LOG_L, int C, int E_ = 16>
-struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))> {
-    using Rx = Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real))>;
+struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
+    using Rx = Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)>;
     using Cx = typename CxT<Real>::T;
     using Rx::E;
     using Rx::L;

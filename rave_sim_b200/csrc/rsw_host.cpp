@@ -334,7 +334,7 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
 template <typename T> static std::vector<T> block_twiddles(int log_l, int rb) {
     std::vector<T> v;
     if (log_l >= 4) {
-        const int max_ls = direct_max_ls(int(2 * sizeof(T)));
+        const int max_ls = direct_max_ls(int(2 * sizeof(T)), log_l);
         for (int s = 0; s < stage_count(log_l, rb) - 1; ++s) {
             for (int64_t k = 0; k < stage_tw_entries(log_l, s, max_ls, rb); ++k) {
                 int64_t m, mod;

@@ -68,7 +68,7 @@ namespace {
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     int off = 0;
-    const int max_ls = direct_max_ls(int(2 * sizeof(T)));
+    const int max_ls = direct_max_ls(int(2 * sizeof(T)), log_l);
     for (int s = 0; s < stage_count(log_l) - 1; ++s) {
         const int count = stage_tw_entries(log_l, s, max_ls);
         for (int k = idx; k < count; k += stride) {

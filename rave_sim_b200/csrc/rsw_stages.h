@@ -29,7 +29,11 @@
 
 namespace rsw {
 
-RSW_HD constexpr int direct_max_ls(int elem_bytes) { return elem_bytes <= 8 ? 9 : 7; }
+// Complex64 blocks of 2^13 (the two-level rows) use the factored form above
+// 2^7 too: their smaller tables let two 512-thread CTAs share an SM.
+RSW_HD constexpr int direct_max_ls(int elem_bytes, int log_l = 0) {
+    return elem_bytes <= 8 && log_l != 13 ? 9 : 7;
+}
 
 // digit width of the kernels with e samples per thread
 RSW_HD constexpr int digit_bits(int e) { return e == 8 ? 3 : 4; }
