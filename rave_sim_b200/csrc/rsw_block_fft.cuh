@@ -30,6 +30,21 @@
 // otherwise two factors W^{(j mod 64) q} * W^{64 (j div 64) q} of 64 and S/64
 // entries per q. FP64 butterflies may take only W^j from the tables and form
 // the other powers as a running product (running()).
+//
+// Complex64 blocks rotate by lifting instead of complex multiplication: a
+// rotation by theta is three shears xr += a xi; xi += b xr; xr += a xi with
+// a = -tan(theta/2), b = sin(theta) (|theta| <= pi/2; a half turn s = -1 is
+// taken out first). Three shears have determinant exactly 1 whatever the
+// rounding of a and b, and the inverse rotation is the same shears with -a,
+// -b in reverse order, so a forward/inverse pair undoes itself up to the
+// rounding of the data. A complex product by the FP32-rounded (cos, sin)
+// scales by |w|^2 = 1 + O(2^-24) instead, the same factor at every split
+// step; over the hundreds of thin split steps of a sample that bias grows
+// linearly and dominated the complex64 detector error (lifting: growth like
+// the square root of the step count, measured 17x smaller after 200 steps in
+// a float32 model of the forward/inverse pair). Table entries of complex64
+// blocks are {a, b, s, 0}; complex128 blocks keep {cos, sin}.
+//
 // Shared memory holds the C sequences with one pad element per E (phys(p):
 // the last stage gives consecutive threads positions E apart, which the pad
 // moves to neighbouring banks) and a per-sequence pitch chosen so that the
@@ -47,6 +62,10 @@ namespace rsw {
 template <typename R> struct CxT;
 template <> struct CxT<double> { using T = double2; };
 template <> struct CxT<float> { using T = float2; };
+// twiddle table entry: {cos, sin} (FP64) or the lifting form {a, b, s, 0} (FP32)
+template <typename R> struct TwT;
+template <> struct TwT<double> { using T = double2; };
+template <> struct TwT<float> { using T = float4; };
 
 __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
 __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
@@ -68,6 +87,39 @@ template <typename C, typename S> __device__ __forceinline__ C cscale(C a, S s) 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+
+// ------------------------------------------------------------ lifting
+// x * exp(i theta) as three shears, a = -tan(theta/2), b = sin(theta)
+__device__ __forceinline__ float2 lift(float2 x, float a, float b) {
+    x.x = __fmaf_rn(a, x.y, x.x);
+    x.y = __fmaf_rn(b, x.x, x.y);
+    x.x = __fmaf_rn(a, x.y, x.x);
+    return x;
+}
+// rotation by a table entry w = {a, b, s, -} (s: half turn, times an optional
+// power-of-two scale, exact) and its inverse (same shears, -a and -b)
+__device__ __forceinline__ float2 rot(float2 x, float4 w) { return lift(cscale(x, w.z), w.x, w.y); }
+__device__ __forceinline__ float2 rot_inv(float2 x, float4 w) { return lift(cscale(x, w.z), -w.x, -w.y); }
+// Lifting form of a unit complex number given in FP64: the half turn goes to
+// s when Re w < 0 (then |theta| <= pi/2 and |a| <= 1); `scale` (a power of
+// two) is folded into s.
+__device__ __forceinline__ float4 lift_of(double2 w, double scale = 1.0) {
+    double sg = scale;
+    if (w.x < 0.0) {
+        w.x = -w.x;
+        w.y = -w.y;
+        sg = -sg;
+    }
+    return make_float4(float(-w.y / (1.0 + w.x)), float(w.y), float(sg), 0.f);
+}
+// multiply by i^q (q mod 4), exact
+template <int Q> __device__ __forceinline__ float2 quarter(float2 x) {
+    constexpr int q = ((Q % 4) + 4) % 4;
+    if constexpr (q == 0) return x;
+    else if constexpr (q == 1) return make_float2(-x.y, x.x);
+    else if constexpr (q == 2) return make_float2(-x.x, -x.y);
+    else return make_float2(x.y, -x.x);
+}
 
 __host__ __device__ constexpr int brev_bits(int q, int bits) {
     int r = 0;
@@ -92,6 +144,42 @@ template <int DIR, typename C> __device__ __forceinline__ C tw16(C x, int e) {
     case 5: return cmul(x, mk(-s1, d * c1));
     case 6: return mk(h * (-x.x - d * x.y), h * (d * x.x - x.y));
     default: return cmul(x, mk(-c1, d * s1));
+    }
+}
+
+// Complex64: the same rotations by lifting. The forward rotation
+// exp(-i pi e / 8) is i^q * exp(i t pi / 8) with |t| <= 2 (t = -e - 4q),
+// applied as the shears of t, then the exact quarter turns; the inverse
+// (DIR = +1) is its exact mirror: the quarter turns back, then the shears
+// with negated coefficients.
+template <int DIR, int EE> __device__ __forceinline__ float2 tw16_lift(float2 x) {
+    constexpr int q = EE <= 2 ? 0 : EE <= 6 ? -1 : -2;
+    constexpr int t = -EE - 4 * q;
+    constexpr float A1 = 0.19891236737965800691f;  // tan(pi/16)
+    constexpr float B1 = 0.38268343236508977173f;  // sin(pi/8)
+    constexpr float A2 = 0.41421356237309504880f;  // tan(pi/8)
+    constexpr float B2 = 0.70710678118654752440f;  // sin(pi/4)
+    constexpr float a = t == -2 ? A2 : t == -1 ? A1 : t == 1 ? -A1 : 0.f;
+    constexpr float b = t == -2 ? -B2 : t == -1 ? -B1 : t == 1 ? B1 : 0.f;
+    if constexpr (DIR < 0) {
+        if constexpr (t != 0) x = lift(x, a, b);
+        return quarter<q>(x);
+    } else {
+        x = quarter<-q>(x);
+        if constexpr (t != 0) x = lift(x, -a, -b);
+        return x;
+    }
+}
+template <int DIR> __device__ __forceinline__ float2 tw16(float2 x, int e) {
+    switch (e) {
+    case 0: return x;
+    case 1: return tw16_lift<DIR, 1>(x);
+    case 2: return tw16_lift<DIR, 2>(x);
+    case 3: return tw16_lift<DIR, 3>(x);
+    case 4: return tw16_lift<DIR, 4>(x);
+    case 5: return tw16_lift<DIR, 5>(x);
+    case 6: return tw16_lift<DIR, 6>(x);
+    default: return tw16_lift<DIR, 7>(x);
     }
 }
 
@@ -157,6 +245,8 @@ template <typename Real, int LOG_L, int C, int E_ = 16>
 struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
     using Rx = Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)>;
     using Cx = typename CxT<Real>::T;
+    using Tw = typename TwT<Real>::T;  // twiddle table entry (16 bytes)
+    static constexpr bool LIFT = sizeof(Real) == 4;  // complex64: rotations by lifting
     using Rx::E;
     using Rx::L;
     using Rx::NS;
@@ -168,7 +258,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
     static constexpr int WANT = (C >= W) ? 1 : W / C;
     static constexpr int PITCH = BASE + (((WANT - BASE) % W) + W) % W;
     static constexpr size_t DATA = size_t(C) * PITCH * sizeof(Cx);
-    static constexpr size_t SMEM = DATA + size_t(Rx::TW) * sizeof(Cx);
+    static constexpr size_t SMEM = DATA + size_t(Rx::TW) * sizeof(Tw);
     static constexpr int RL = 1 << Rx::lr(NS - 1);  // radix of the last stage
 
     __device__ static __forceinline__ int phys(int p) { return p + (p >> LOG_E); }
@@ -201,8 +291,8 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
             for (int q = 0; q < R; ++q) v[reg<s, BR>(i, q)] = sm[phys(pos<s>(tp, i, q))];
     }
 
-    // twiddle W_{RS}^{j q} of stage s from the shared-memory tables
-    template <int s> __device__ static __forceinline__ Cx twid(const Cx *tw, int j, int q) {
+    // twiddle W_{RS}^{j q} of stage s from the shared-memory tables (complex128)
+    template <int s> __device__ static __forceinline__ Cx twid(const Tw *tw, int j, int q) {
         constexpr int LSS = Rx::ls(s);
         const Cx *t = tw + Rx::twoff(s);
         if constexpr (Rx::direct(s)) {
@@ -212,6 +302,23 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
             const Cx a = t[(q - 1) * 64 + (j & 63)];
             const Cx b = t[(R - 1) * 64 + (q - 1) * (1 << (LSS - 6)) + (j >> 6)];
             return cmul(a, b);
+        }
+    }
+    // complex64: x * W_{RS}^{j q} (INV: x * conj(W)) by lifting; a factored
+    // twiddle is two rotations, undone in reverse order by the inverse
+    template <int s, bool INV> __device__ static __forceinline__ Cx twlift(const Tw *tw, int j, int q, Cx x) {
+        constexpr int LSS = Rx::ls(s);
+        const Tw *t = tw + Rx::twoff(s);
+        if constexpr (Rx::direct(s)) {
+            const Tw w = t[((q - 1) << LSS) + j];
+            return INV ? rot_inv(x, w) : rot(x, w);
+        } else {
+            constexpr int R = 1 << Rx::lr(s);
+            const Tw a = t[(q - 1) * 64 + (j & 63)];
+            const Tw b = t[(R - 1) * 64 + (q - 1) * (1 << (LSS - 6)) + (j >> 6)];
+            x = cscale(x, a.z * b.z);
+            if constexpr (INV) return lift(lift(x, -b.x, -b.y), -a.x, -a.y);
+            else return lift(lift(x, a.x, a.y), b.x, b.y);
         }
     }
 
@@ -227,7 +334,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
     }
 
     // forward stage s: natural in -> radix-R DFT -> bit-reversed out, twiddled
-    template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Cx *tw) {
+    template <int s> __device__ static __forceinline__ void dif(int tp, Cx *v, const Tw *tw) {
         constexpr int R = 1 << Rx::lr(s);
         constexpr int LSS = Rx::ls(s);
 #pragma unroll
@@ -248,14 +355,15 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
 #pragma unroll
                     for (int q = 1; q < R; ++q) {
                         Cx &x = v[reg<s, true>(i, q)];
-                        x = cmul(x, twid<s>(tw, j, q));
+                        if constexpr (LIFT) x = twlift<s, false>(tw, j, q, x);
+                        else x = cmul(x, twid<s>(tw, j, q));
                     }
                 }
             }
         }
     }
     // inverse stage s: bit-reversed in -> conjugate twiddle -> inverse DFT -> natural out
-    template <int s> __device__ static __forceinline__ void dit(int tp, Cx *v, const Cx *tw) {
+    template <int s> __device__ static __forceinline__ void dit(int tp, Cx *v, const Tw *tw) {
         constexpr int R = 1 << Rx::lr(s);
         constexpr int LSS = Rx::ls(s);
 #pragma unroll
@@ -275,7 +383,8 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
 #pragma unroll
                     for (int q = 1; q < R; ++q) {
                         Cx &x = v[reg<s, true>(i, q)];
-                        x = cmulc(x, twid<s>(tw, j, q));
+                        if constexpr (LIFT) x = twlift<s, true>(tw, j, q, x);
+                        else x = cmulc(x, twid<s>(tw, j, q));
                     }
                 }
             }
@@ -307,7 +416,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
 
     // Full forward transform from stage-0 positions (natural layout) to
     // last-stage positions (bit-reversed layout) in registers.
-    template <int s = 0> __device__ static __forceinline__ void forward(Cx *sm, int tp, Cx *v, const Cx *tw) {
+    template <int s = 0> __device__ static __forceinline__ void forward(Cx *sm, int tp, Cx *v, const Tw *tw) {
         dif<s>(tp, v, tw);
         if constexpr (s < NS - 1) {
             st<s, true>(sm, tp, v);
@@ -318,7 +427,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
     }
     // Full inverse transform from last-stage positions (bit-reversed layout)
     // to stage-0 positions (natural layout).
-    template <int s = NS - 1> __device__ static __forceinline__ void inverse(Cx *sm, int tp, Cx *v, const Cx *tw) {
+    template <int s = NS - 1> __device__ static __forceinline__ void inverse(Cx *sm, int tp, Cx *v, const Tw *tw) {
         dit<s>(tp, v, tw);
         if constexpr (s > 0) {
             st<s, false>(sm, tp, v);
@@ -348,7 +457,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
     __device__ static __forceinline__ int last_freq(int tp, int r) { return freq_base(tp) | freq_off(r); }
 
     // copy the block's twiddle tables (global, host-built layout) into shared memory
-    __device__ static __forceinline__ void load_twiddles(Cx *tw_sm, const Cx *__restrict__ tw_g) {
+    __device__ static __forceinline__ void load_twiddles(Tw *tw_sm, const Tw *__restrict__ tw_g) {
         for (int k = threadIdx.x; k < Rx::TW; k += NT) tw_sm[k] = tw_g[k];
     }
 };

@@ -328,22 +328,52 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
     v.push_back(T(c.imag()));
 }
 
+// Lifting form {a, b, s, 0} of W_M^m = exp(-2 pi i m / M) for complex64
+// tables (rotation by three shears, rsw_block_fft.cuh): m is reduced to
+// (-M/2, M/2]; beyond a quarter turn the half turn goes to s = -1, so that the
+// remaining angle t = -2 pi m' / M has |t| <= pi/2; a = -tan(t/2), b = sin(t).
+static void push_lift(std::vector<float> &v, int64_t m, int64_t M) {
+    m %= M;
+    if (m < 0) m += M;
+    if (m > M / 2) m -= M;
+    float sg = 1.f;
+    if (4 * m > M) {
+        m -= M / 2;
+        sg = -1.f;
+    } else if (4 * m < -M) {
+        m += M / 2;
+        sg = -1.f;
+    }
+    const long double pi = 3.14159265358979323846264338327950288L;
+    const long double t = -2.0L * pi * (long double)m / (long double)M;
+    v.push_back(float(-tanl(t / 2)));
+    v.push_back(float(sinl(t)));
+    v.push_back(sg);
+    v.push_back(0.f);
+}
+
 // Block twiddle tables of a block of length 2^log_l in the shared-memory
 // layout of the block FFT (rsw_stages.h): stages in order, entry k of stage s
-// is W_{RS}^m with (m, RS) from stage_tw_entry.
+// is W_{RS}^m with (m, RS) from stage_tw_entry; 16 bytes per entry ({cos, sin}
+// in FP64, or the complex64 lifting form).
 template <typename T> static std::vector<T> block_twiddles(int log_l, int rb) {
     std::vector<T> v;
+    constexpr bool lift = sizeof(T) == 4;
     if (log_l >= 4) {
         const int max_ls = direct_max_ls(int(2 * sizeof(T)), log_l);
         for (int s = 0; s < stage_count(log_l, rb) - 1; ++s) {
             for (int64_t k = 0; k < stage_tw_entries(log_l, s, max_ls, rb); ++k) {
                 int64_t m, mod;
                 stage_tw_entry(log_l, s, max_ls, rb, k, &m, &mod);
-                push_c(v, twiddle(m, mod));
+                if constexpr (lift) push_lift(v, m, mod);
+                else push_c(v, twiddle(m, mod));
             }
         }
     }
-    if (v.empty()) push_c(v, cplx(1, 0));
+    if (v.empty()) {
+        if constexpr (lift) push_lift(v, 0, 1);
+        else push_c(v, cplx(1, 0));
+    }
     return v;
 }
 
@@ -896,7 +926,7 @@ rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, dou
     a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0);
     const bool two = p->log_n1 > 0;
     if (two && a.pr.has_h) {
-        CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_nr) * p->elem()));
+        CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_nr) * 16));  // 16-byte entries
         CHECK(prepare_chirp(p, a.pr, p->h3_call.p, s));
     }
     a.in = u;
@@ -1251,7 +1281,7 @@ struct Runner {
         if (fresh) {
             chirp_dz.push_back(dz);
             if (S->h3_pool.size() <= slot) S->h3_pool.emplace_back(new DevBuf());
-            CHECK(S->h3_pool[slot]->alloc(size_t(int64_t(1) << P->log_nr) * P->elem()));
+            CHECK(S->h3_pool[slot]->alloc(size_t(int64_t(1) << P->log_nr) * 16));  // 16-byte entries
             CHECK(prepare_chirp(P, pr, S->h3_pool[slot]->p, st));
             return RSW_OK;
         }

@@ -63,8 +63,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[1536 * 1024];
 namespace {
 
 // Block twiddles of a block of length 2^log_l into `out` in the layout of
-// the block FFT (rsw_stages.h); W_M^m = exp(-2 pi i m / M) from sincospi of
-// an exact argument.
+// the block FFT (rsw_stages.h), 16 bytes per entry: W_M^m = exp(-2 pi i m / M)
+// as {cos, sin} (FP64) from sincospi of an exact argument, or for complex64
+// the lifting form {a, b, s, 0}: m reduced to (-M/2, M/2], a half turn taken
+// out into s beyond a quarter turn, then a = -tan(t/2), b = sin(t) of the
+// remaining angle t = -2 pi m' / M.
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     int off = 0;
@@ -74,10 +77,29 @@ __device__ void block_tables(T *out, int log_l, int idx, int stride) {
         for (int k = idx; k < count; k += stride) {
             int64_t m, mod;
             stage_tw_entry(log_l, s, max_ls, 4, k, &m, &mod);
-            double sn, cs;
-            sincospi(-2.0 * double(m % mod) / double(mod), &sn, &cs);
-            out[2 * (off + k)] = T(cs);
-            out[2 * (off + k) + 1] = T(sn);
+            if constexpr (sizeof(T) == 8) {
+                double sn, cs;
+                sincospi(-2.0 * double(m % mod) / double(mod), &sn, &cs);
+                out[2 * (off + k)] = T(cs);
+                out[2 * (off + k) + 1] = T(sn);
+            } else {
+                m %= mod;
+                if (m > mod / 2) m -= mod;
+                float sg = 1.f;
+                if (4 * m > mod) {
+                    m -= mod / 2;
+                    sg = -1.f;
+                } else if (4 * m < -mod) {
+                    m += mod / 2;
+                    sg = -1.f;
+                }
+                double sh, ch;
+                sincospi(double(m) / double(mod), &sh, &ch);  // angle -t/2
+                out[4 * (off + k)] = T(sh / ch);                          // -tan(t/2)
+                out[4 * (off + k) + 1] = T(-sinpi(2.0 * double(m) / double(mod)));  // sin(t)
+                out[4 * (off + k) + 2] = sg;
+                out[4 * (off + k) + 3] = 0.f;
+            }
         }
         off += count;
     }

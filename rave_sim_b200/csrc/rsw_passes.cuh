@@ -261,14 +261,14 @@ __device__ __forceinline__ double2 prop_apply(const PropArgs &p, int64_t k, int6
     const double2 H = make_double2(p.A.x * c - p.A.y * s, p.A.x * s + p.A.y * c);
     return cmul(U, H);
 }
+// complex64: the transfer function in FP64, applied by lifting (no
+// amplitude bias from rounding H to FP32)
 __device__ __forceinline__ float2 prop_apply(const PropArgs &p, int64_t k, int64_t ks, float2 U) {
     if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) return make_float2(0.f, 0.f);
     if (!p.has_h) return U;
-    float s, c;
-    sincosf(float(reduce_phase(prop_phase(p, ks))), &s, &c);
-    const float ax = float(p.A.x), ay = float(p.A.y);
-    const float2 H = make_float2(ax * c - ay * s, ax * s + ay * c);
-    return cmul(U, H);
+    double s, c;
+    sincos_phase(prop_phase(p, ks), &s, &c);
+    return rot(U, lift_of(make_double2(p.A.x * c - p.A.y * s, p.A.x * s + p.A.y * c)));
 }
 
 template <typename Cx> __device__ __forceinline__ Cx one_c();
@@ -300,8 +300,9 @@ __device__ __forceinline__ int k2_bound(int64_t x, int log_n1, int l) {
 
 // Layout of the column kernel's four-step factors (one copy per tile
 // parity): per column, the thread-part factors X (2^LX, stride XP) and Y
-// (2^LY, stride YP) in FP64, then the E register parts (stride E + 1) in the
-// field's precision. T = threads per column.
+// (2^LY, stride YP) in FP64, then the E register parts (stride E + 1) as
+// 16-byte twiddle entries ({cos, sin} in FP64, or the complex64 lifting
+// form). T = threads per column.
 template <int T> struct ColTab {
     static constexpr int LOG_T = ilog2(T);
     static constexpr int LX = (LOG_T + 1) / 2, LY = LOG_T - LX;
@@ -332,15 +333,16 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
     using Cx = typename B::Cx;
     constexpr int L = B::L;
     constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
+    using Tw = typename B::Tw;
     extern __shared__ __align__(16) unsigned char smraw[];
     Cx *sm = reinterpret_cast<Cx *>(smraw);
-    Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
+    Tw *tw = reinterpret_cast<Tw *>(smraw + B::DATA);
     constexpr int NQ = (L >> 6) > 1 ? (L >> 6) : 2;  // k2s >> 6 spans [-NQ/2, NQ/2)
     constexpr int NCH = 64 + NQ + E;  // chirp factors per row: P, Q and the per-register R
     const int tp = threadIdx.x;
     const int flags = a.flags;
     const int64_t rows = a.n >> LOG_L2;
-    B::load_twiddles(tw, static_cast<const Cx *>(a.tw_row));
+    B::load_twiddles(tw, static_cast<const Tw *>(a.tw_row));
     __syncthreads();
     const int64_t nmask = (int64_t(1) << a.tw_log) - 1;
     const double tw_scale = a.tw_scale;
@@ -356,9 +358,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
     for (int64_t row = blockIdx.x; row < rows; row += gridDim.x, parity ^= 1) {
         // per-row tables, double-buffered by row parity: the next row fills
         // the other copy while slower warps still read this one
-        Cx *vec = tw + B::TW + parity * (NV + NCH);  // four-step factors: [0,64) low, [64, NV) high
+        // 16-byte entries; complex64 keeps the lifting form {a, b, s, 0} of
+        // each factor, except P and Q, kept in FP64 (their product is taken once
+        // per row and thread before it is turned into a rotation)
+        Tw *vec = tw + B::TW + parity * (NV + NCH);  // four-step factors: [0,64) low, [64, NV) high
         // chirp factors: [0,64) P[a], [64, 64+NQ) Q[b + NQ/2], [64+NQ, NCH) R[r]
-        Cx *chp = vec + NV;
+        Tw *chp = vec + NV;
         // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
         // conjugate four-step twiddle of the innermost split uses tw_k
         // (rows beyond one transform belong to the next one of a batch)
@@ -388,7 +393,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                     const int64_t sr = (fo & (L >> 1)) ? int64_t(fo) - L : int64_t(fo);
                     w = cis_turns(frac_dd(g1h, g1l, double(kbase * sr)));
                 }
-                chp[idx] = cvt(w, Cx{});
+                if constexpr (B::LIFT) {
+                    if (idx < 64 + NQ) reinterpret_cast<double2 *>(chp)[idx] = w;
+                    else chp[idx] = lift_of(w);
+                } else {
+                    chp[idx] = w;
+                }
             }
         }
         if (flags & (PF_TW | PF_TWF)) {
@@ -397,8 +407,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 const int64_t m = ((idx < 64 ? int64_t(idx) : int64_t(idx - 64) << 6) * tw_k) & nmask;
                 double2 w = w4(a, m);
                 w = make_double2(w.x, -w.y);
-                if (idx >= 64) w = make_double2(w.x * tw_scale, w.y * tw_scale);
-                vec[idx] = cvt(w, Cx{});
+                if constexpr (B::LIFT) {
+                    vec[idx] = lift_of(w, idx >= 64 ? tw_scale : 1.0);
+                } else {
+                    if (idx >= 64) w = make_double2(w.x * tw_scale, w.y * tw_scale);
+                    vec[idx] = w;
+                }
             }
         }
         if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
@@ -423,7 +437,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int n2 = B::first_pos(tp, r);
-                    v[r] = cmulc(cmulc(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                    if constexpr (B::LIFT) {  // the exact inverse of the PF_TW rotations below
+                        const Tw lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
+                        v[r] = lift(lift(cscale(v[r], lo.z * hi.z), -hi.x, -hi.y), -lo.x, -lo.y);
+                    } else {
+                        v[r] = cmulc(cmulc(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                    }
                 }
             }
             // Rows of multi-level plans never transmit (the column pass does).
@@ -455,7 +474,21 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 // H = P[fbase & 63] * Q[fbase >> 6] * R[r] * h3[r][tp]; k2 >= L/2
                 // (k2s = k2 - L) is decided by the compile-time part of the
                 // frequency, so 0 <= fbase < L/2
-                const Cx *h3 = static_cast<const Cx *>(a.pr.h3);
+                const Tw *h3 = static_cast<const Tw *>(a.pr.h3);
+                if constexpr (B::LIFT) {
+                    // three rotations: the thread's P Q (FP64 product), R[r], h3
+                    const double2 *chd = reinterpret_cast<const double2 *>(chp);
+                    const Tw tl = lift_of(cmul(chd[fbase & 63], chd[64 + (fbase >> 6) + NQ / 2]));
+#pragma unroll
+                    for (int r = 0; r < E; ++r) {
+                        const int k2 = fbase | B::freq_off(r);
+                        const Tw rr = chp[64 + NQ + r], g = __ldg(h3 + r * B::T + tp);
+                        Cx x = cscale(v[r], tl.z * rr.z * g.z);
+                        x = lift(lift(lift(x, tl.x, tl.y), rr.x, rr.y), g.x, g.y);
+                        v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : x;
+                        if (r % 4 == 3) asm volatile("" ::: "memory");
+                    }
+                } else {
                 const Cx tb = cmul(chp[fbase & 63], chp[64 + (fbase >> 6) + NQ / 2]);
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
@@ -467,6 +500,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                     // complex64 row spilled 132 bytes per thread instead of 52,
                     // 5 % slower)
                     if (r % 4 == 3) asm volatile("" ::: "memory");
+                }
                 }
             } else {
 #pragma unroll
@@ -492,7 +526,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int n2 = B::first_pos(tp, r);
-                    v[r] = cmul(cmul(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                    if constexpr (B::LIFT) {
+                        const Tw lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
+                        v[r] = lift(lift(cscale(v[r], lo.z * hi.z), lo.x, lo.y), hi.x, hi.y);
+                    } else {
+                        v[r] = cmul(cmul(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
+                    }
                 }
             } else if (flags & PF_SCALE) {
                 const Real f = Real(a.pr.fac);
@@ -521,22 +560,25 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     // permutation, so the thread part is X[tp & (2^LX - 1)] * Y[tp >> LX] with
     // X[i] = W^(n2 freq_base(i)), Y[j] = W^(n2 freq_base(j 2^LX)), multiplied
     // in FP64. The strides put the C columns of a wavefront in different banks.
+    // complex64 applies both parts as rotations by lifting (register parts
+    // stored in the lifting form).
+    using Tw = typename B::Tw;
     using CT = ColTab<B::T>;
     constexpr int LX = CT::LX, NX = 1 << LX, NXY = NX + (1 << CT::LY);
     constexpr int XP = CT::XP, YP = CT::YP, EP = E + 1;
-    constexpr size_t PAR = CT::template parity_bytes<C, E, int(sizeof(Cx))>();
+    constexpr size_t PAR = CT::template parity_bytes<C, E, int(sizeof(Tw))>();
     extern __shared__ __align__(16) unsigned char smraw[];
     const int t = threadIdx.x;
     const int c = t % C;
     const int tp = t / C;
     Cx *sm = reinterpret_cast<Cx *>(smraw) + c * B::PITCH;
-    Cx *tw = reinterpret_cast<Cx *>(smraw + B::DATA);
+    Tw *tw = reinterpret_cast<Tw *>(smraw + B::DATA);
     const int log_n2 = a.log_n2;
     const int flags = a.flags;
     const int log_tb = log_n2 - ilog2(C);  // tiles per batch: 2^log_tb
     const int64_t tiles = (a.n >> LOG_L1) / C;
     const int64_t nmask = (int64_t(1) << a.tw_log) - 1;
-    B::load_twiddles(tw, static_cast<const Cx *>(a.tw_col));
+    B::load_twiddles(tw, static_cast<const Tw *>(a.tw_col));
     __syncthreads();
     // An inverse + forward tile starts and ends with the last-stage positions
     // of each thread, so the next tile may overwrite the data buffer without
@@ -550,7 +592,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         // factor tables, double-buffered by tile parity
         double2 *tx = reinterpret_cast<double2 *>(tab0 + parity * PAR);
         double2 *ty = tx + C * XP;
-        Cx *vec = reinterpret_cast<Cx *>(ty + C * YP);
+        Tw *vec = reinterpret_cast<Tw *>(ty + C * YP);
         const int64_t batch = tile >> log_tb;
         const int64_t col0 = (tile & ((int64_t(1) << log_tb) - 1)) * C;  // column within the batch
         const int64_t col = col0 + c;
@@ -563,8 +605,10 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
                     tx[cc * XP + e] = w4(a, (int64_t(B::freq_base(e)) * n2) & nmask);
                 else if (e < NXY)
                     ty[cc * YP + (e - NX)] = w4(a, (int64_t(B::freq_base((e - NX) << LX)) * n2) & nmask);
+                else if constexpr (B::LIFT)
+                    vec[cc * EP + (e - NXY)] = lift_of(w4(a, (int64_t(B::freq_off(e - NXY)) * n2) & nmask));
                 else
-                    vec[cc * EP + (e - NXY)] = cvt(w4(a, (int64_t(B::freq_off(e - NXY)) * n2) & nmask), Cx{});
+                    vec[cc * EP + (e - NXY)] = w4(a, (int64_t(B::freq_off(e - NXY)) * n2) & nmask);
             }
         }
         if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
@@ -576,11 +620,20 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
             for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
             if (flags & PF_TWI) {
                 __syncthreads();  // this tile's factor table is complete
-                const Cx *vc = vec + c * EP;
-                const Cx w = cvt(cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]), Cx{});
+                const Tw *vc = vec + c * EP;
+                const double2 w64 = cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]);
                 const Real s = Real(a.tw_scale);  // a power of two: exact
+                if constexpr (B::LIFT) {
+                    // the exact inverse of the PF_TW rotations (register part first)
+                    const Tw wt = lift_of(w64);
 #pragma unroll
-                for (int r = 0; r < E; ++r) v[r] = cscale(cmulc(v[r], cmul(w, vc[r])), s);
+                    for (int r = 0; r < E; ++r)
+                        v[r] = lift(lift(cscale(v[r], wt.z * vc[r].z * s), -vc[r].x, -vc[r].y), -wt.x, -wt.y);
+                } else {
+                    const Cx w = cvt(w64, Cx{});
+#pragma unroll
+                    for (int r = 0; r < E; ++r) v[r] = cscale(cmulc(v[r], cmul(w, vc[r])), s);
+                }
             }
             B::inverse(sm, tp, v, tw);
         } else {
@@ -593,10 +646,18 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
-                const Cx *vc = vec + c * EP;
-                const Cx w = cvt(cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]), Cx{});
+                const Tw *vc = vec + c * EP;
+                const double2 w64 = cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]);
+                if constexpr (B::LIFT) {
+                    const Tw wt = lift_of(w64);
 #pragma unroll
-                for (int r = 0; r < E; ++r) v[r] = cmul(v[r], cmul(w, vc[r]));
+                    for (int r = 0; r < E; ++r)
+                        v[r] = lift(lift(cscale(v[r], wt.z * vc[r].z), wt.x, wt.y), vc[r].x, vc[r].y);
+                } else {
+                    const Cx w = cvt(w64, Cx{});
+#pragma unroll
+                    for (int r = 0; r < E; ++r) v[r] = cmul(v[r], cmul(w, vc[r]));
+                }
             }
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[int64_t(B::last_pos(tp, r)) << log_n2] = v[r];
@@ -609,9 +670,10 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 }
 
 // exp(2 pi i G N1^2 k2s^2) for every register (r, tp) of the row kernel
-// Block<Real, LOG_L2, 1, E>, stored at r * T + tp.
+// Block<Real, LOG_L2, 1, E>, stored at r * T + tp ({cos, sin} for complex128,
+// the lifting form for complex64).
 template <typename Real, int LOG_L2, int E>
-__global__ void chirp_table_kernel(typename CxT<Real>::T *__restrict__ out, double g3_hi, double g3_lo) {
+__global__ void chirp_table_kernel(typename TwT<Real>::T *__restrict__ out, double g3_hi, double g3_lo) {
     using B = Block<Real, LOG_L2, 1, E>;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= B::L) return;
@@ -619,7 +681,9 @@ __global__ void chirp_table_kernel(typename CxT<Real>::T *__restrict__ out, doub
     const int half2 = 1 << (LOG_L2 - 1);
     const int k2 = B::last_freq(tp, r);
     const double k2s = double(k2 >= half2 ? k2 - 2 * half2 : k2);
-    out[idx] = cvt(cis_turns(frac_dd(g3_hi, g3_lo, k2s * k2s)), typename CxT<Real>::T{});
+    const double2 w = cis_turns(frac_dd(g3_hi, g3_lo, k2s * k2s));
+    if constexpr (sizeof(Real) == 4) out[idx] = lift_of(w);
+    else out[idx] = w;
 }
 
 void count_launch();
@@ -644,7 +708,7 @@ template <int L, int E> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L
 template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
     auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
-    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * sizeof(typename B::Cx);
+    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * sizeof(typename B::Tw);
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
@@ -675,7 +739,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
     auto k = col_pass_kernel<Real, LG, C, E>;
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
-    const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, int(sizeof(typename B::Cx))>();
+    const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, int(sizeof(typename B::Tw))>();
     static cudaError_t attr = prep(k, tab);
     if (attr != cudaSuccess) return attr;
     static int64_t cap_tab = resident_ctas(k, B::NT, tab);
@@ -691,7 +755,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
 
 template <typename Real, int LG, int E> static cudaError_t chirp_impl(void *out, double hi, double lo, cudaStream_t s) {
     chirp_table_kernel<Real, LG, E><<<((1 << LG) + 255) / 256, 256, 0, s>>>(
-        static_cast<typename CxT<Real>::T *>(out), hi, lo);
+        static_cast<typename TwT<Real>::T *>(out), hi, lo);
     count_launch();
     return cudaGetLastError();
 }
