@@ -43,7 +43,10 @@
 // linearly and dominated the complex64 detector error (lifting: growth like
 // the square root of the step count, measured 17x smaller after 200 steps in
 // a float32 model of the forward/inverse pair). Table entries of complex64
-// blocks are {a, b, s, 0}; complex128 blocks keep {cos, sin}.
+// blocks are {a, b} with the half turn in the lowest mantissa bit of a (a is
+// rounded to the nearest float of that parity: the rotation angle moves by
+// at most one ulp of a, the same in the forward and the inverse pass, and the
+// shears keep determinant 1); complex128 blocks keep {cos, sin}.
 //
 // Shared memory holds the C sequences with one pad element per E (phys(p):
 // the last stage gives consecutive threads positions E apart, which the pad
@@ -62,10 +65,16 @@ namespace rsw {
 template <typename R> struct CxT;
 template <> struct CxT<double> { using T = double2; };
 template <> struct CxT<float> { using T = float2; };
-// twiddle table entry: {cos, sin} (FP64) or the lifting form {a, b, s, 0} (FP32)
+// block twiddle table entry: {cos, sin} (FP64) or the lifting form {a, b}
+// with the half turn in the low bit of a (FP32)
 template <typename R> struct TwT;
 template <> struct TwT<double> { using T = double2; };
-template <> struct TwT<float> { using T = float4; };
+template <> struct TwT<float> { using T = float2; };
+// 16-byte entry of the per-row and per-tile factor tables and of the chirp
+// table: {cos, sin} (FP64) or the lifting form {a, b, s, 0} (FP32)
+template <typename R> struct LiftT;
+template <> struct LiftT<double> { using T = double2; };
+template <> struct LiftT<float> { using T = float4; };
 
 __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
 __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
@@ -96,13 +105,16 @@ __device__ __forceinline__ float2 lift(float2 x, float a, float b) {
     x.x = __fmaf_rn(a, x.y, x.x);
     return x;
 }
-// rotation by a table entry w = {a, b, s, -} (s: half turn, times an optional
-// power-of-two scale, exact) and its inverse (same shears, -a and -b)
+// rotation by a 16-byte factor-table entry w = {a, b, s, -} (s: half turn,
+// times an optional power-of-two scale, exact) and its inverse (same shears,
+// -a and -b)
 __device__ __forceinline__ float2 rot(float2 x, float4 w) { return lift(cscale(x, w.z), w.x, w.y); }
 __device__ __forceinline__ float2 rot_inv(float2 x, float4 w) { return lift(cscale(x, w.z), -w.x, -w.y); }
 // Lifting form of a unit complex number given in FP64: the half turn goes to
 // s when Re w < 0 (then |theta| <= pi/2 and |a| <= 1); `scale` (a power of
-// two) is folded into s.
+// two) is folded into s. a = -Im w / (1 + Re w) with 1 + Re w in [1, 2]: the
+// FP32 reciprocal refined by one Newton step in FP64 (relative error below
+// 1e-14, then a single rounding to FP32), a few registers and no division.
 __device__ __forceinline__ float4 lift_of(double2 w, double scale = 1.0) {
     double sg = scale;
     if (w.x < 0.0) {
@@ -110,8 +122,21 @@ __device__ __forceinline__ float4 lift_of(double2 w, double scale = 1.0) {
         w.y = -w.y;
         sg = -sg;
     }
-    return make_float4(float(-w.y / (1.0 + w.x)), float(w.y), float(sg), 0.f);
+    const double d = 1.0 + w.x;
+    double r = double(__frcp_rn(float(d)));
+    r = fma(r, fma(-d, r, 1.0), r);
+    return make_float4(float(-w.y * r), float(w.y), float(sg), 0.f);
 }
+// +-1.0f from the half-turn bit of a packed block twiddle {a, b} (the low bit
+// of a), and the product of the half turns of two entries
+__device__ __forceinline__ float half_turn(float a) {
+    return __uint_as_float((__float_as_uint(a) << 31) | 0x3f800000u);
+}
+__device__ __forceinline__ float half_turn2(float a, float b) {
+    return __uint_as_float(((__float_as_uint(a) ^ __float_as_uint(b)) << 31) | 0x3f800000u);
+}
+__device__ __forceinline__ float2 rot(float2 x, float2 w) { return lift(cscale(x, half_turn(w.x)), w.x, w.y); }
+__device__ __forceinline__ float2 rot_inv(float2 x, float2 w) { return lift(cscale(x, half_turn(w.x)), -w.x, -w.y); }
 // multiply by i^q (q mod 4), exact
 template <int Q> __device__ __forceinline__ float2 quarter(float2 x) {
     constexpr int q = ((Q % 4) + 4) % 4;
@@ -316,7 +341,7 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
             constexpr int R = 1 << Rx::lr(s);
             const Tw a = t[(q - 1) * 64 + (j & 63)];
             const Tw b = t[(R - 1) * 64 + (q - 1) * (1 << (LSS - 6)) + (j >> 6)];
-            x = cscale(x, a.z * b.z);
+            x = cscale(x, half_turn2(a.x, b.x));
             if constexpr (INV) return lift(lift(x, -b.x, -b.y), -a.x, -a.y);
             else return lift(lift(x, a.x, a.y), b.x, b.y);
         }

@@ -328,28 +328,33 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
     v.push_back(T(c.imag()));
 }
 
-// Lifting form {a, b, s, 0} of W_M^m = exp(-2 pi i m / M) for complex64
-// tables (rotation by three shears, rsw_block_fft.cuh): m is reduced to
-// (-M/2, M/2]; beyond a quarter turn the half turn goes to s = -1, so that the
+// Packed lifting form {a, b} of W_M^m = exp(-2 pi i m / M) for complex64
+// block tables (rotation by three shears, rsw_block_fft.cuh): m is reduced to
+// (-M/2, M/2]; beyond a quarter turn a half turn is taken out, so that the
 // remaining angle t = -2 pi m' / M has |t| <= pi/2; a = -tan(t/2), b = sin(t).
+// The half turn is the lowest mantissa bit of a: a is rounded to the nearest
+// float whose low bit is the half-turn flag.
 static void push_lift(std::vector<float> &v, int64_t m, int64_t M) {
     m %= M;
     if (m < 0) m += M;
     if (m > M / 2) m -= M;
-    float sg = 1.f;
+    unsigned flip = 0;
     if (4 * m > M) {
         m -= M / 2;
-        sg = -1.f;
+        flip = 1;
     } else if (4 * m < -M) {
         m += M / 2;
-        sg = -1.f;
+        flip = 1;
     }
     const long double pi = 3.14159265358979323846264338327950288L;
     const long double t = -2.0L * pi * (long double)m / (long double)M;
-    v.push_back(float(-tanl(t / 2)));
+    const long double a = -tanl(t / 2);
+    float af = float(a);
+    uint32_t bits;
+    std::memcpy(&bits, &af, 4);
+    if ((bits & 1u) != flip) af = std::nextafter(af, (long double)af < a ? HUGE_VALF : -HUGE_VALF);
+    v.push_back(af);
     v.push_back(float(sinl(t)));
-    v.push_back(sg);
-    v.push_back(0.f);
 }
 
 // Block twiddle tables of a block of length 2^log_l in the shared-memory

@@ -63,11 +63,12 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[1536 * 1024];
 namespace {
 
 // Block twiddles of a block of length 2^log_l into `out` in the layout of
-// the block FFT (rsw_stages.h), 16 bytes per entry: W_M^m = exp(-2 pi i m / M)
-// as {cos, sin} (FP64) from sincospi of an exact argument, or for complex64
-// the lifting form {a, b, s, 0}: m reduced to (-M/2, M/2], a half turn taken
-// out into s beyond a quarter turn, then a = -tan(t/2), b = sin(t) of the
-// remaining angle t = -2 pi m' / M.
+// the block FFT (rsw_stages.h): W_M^m = exp(-2 pi i m / M) as {cos, sin}
+// (FP64) from sincospi of an exact argument, or for complex64 the packed
+// lifting form {a, b}: m reduced to (-M/2, M/2], a half turn taken out beyond
+// a quarter turn, a = -tan(t/2), b = sin(t) of the remaining angle
+// t = -2 pi m' / M, and a rounded to the nearest float whose lowest mantissa
+// bit is the half-turn flag (the rule of the host-built tables).
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     int off = 0;
@@ -85,20 +86,21 @@ __device__ void block_tables(T *out, int log_l, int idx, int stride) {
             } else {
                 m %= mod;
                 if (m > mod / 2) m -= mod;
-                float sg = 1.f;
+                unsigned flip = 0;
                 if (4 * m > mod) {
                     m -= mod / 2;
-                    sg = -1.f;
+                    flip = 1;
                 } else if (4 * m < -mod) {
                     m += mod / 2;
-                    sg = -1.f;
+                    flip = 1;
                 }
                 double sh, ch;
                 sincospi(double(m) / double(mod), &sh, &ch);  // angle -t/2
-                out[4 * (off + k)] = T(sh / ch);                          // -tan(t/2)
-                out[4 * (off + k) + 1] = T(-sinpi(2.0 * double(m) / double(mod)));  // sin(t)
-                out[4 * (off + k) + 2] = sg;
-                out[4 * (off + k) + 3] = 0.f;
+                const double a = sh / ch;                       // -tan(t/2)
+                float af = float(a);
+                if ((__float_as_uint(af) & 1u) != flip) af = nextafterf(af, double(af) < a ? HUGE_VALF : -HUGE_VALF);
+                out[2 * (off + k)] = af;
+                out[2 * (off + k) + 1] = T(-sinpi(2.0 * double(m) / double(mod)));  // sin(t)
             }
         }
         off += count;

@@ -334,9 +334,11 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
     constexpr int L = B::L;
     constexpr int NV = 64 + (L >> 6 > 0 ? L >> 6 : 1);
     using Tw = typename B::Tw;
+    using Lf = typename LiftT<Real>::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     Cx *sm = reinterpret_cast<Cx *>(smraw);
     Tw *tw = reinterpret_cast<Tw *>(smraw + B::DATA);
+    Lf *const tabs = reinterpret_cast<Lf *>(smraw + (B::SMEM + 15) / 16 * 16);
     constexpr int NQ = (L >> 6) > 1 ? (L >> 6) : 2;  // k2s >> 6 spans [-NQ/2, NQ/2)
     constexpr int NCH = 64 + NQ + E;  // chirp factors per row: P, Q and the per-register R
     const int tp = threadIdx.x;
@@ -361,9 +363,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
         // 16-byte entries; complex64 keeps the lifting form {a, b, s, 0} of
         // each factor, except P and Q, kept in FP64 (their product is taken once
         // per row and thread before it is turned into a rotation)
-        Tw *vec = tw + B::TW + parity * (NV + NCH);  // four-step factors: [0,64) low, [64, NV) high
+        Lf *vec = tabs + parity * (NV + NCH);  // four-step factors: [0,64) low, [64, NV) high
         // chirp factors: [0,64) P[a], [64, 64+NQ) Q[b + NQ/2], [64+NQ, NCH) R[r]
-        Tw *chp = vec + NV;
+        Lf *chp = vec + NV;
         // row -> (p1, pb): spectrum index base kbase = k1 + N1 kb; the
         // conjugate four-step twiddle of the innermost split uses tw_k
         // (rows beyond one transform belong to the next one of a batch)
@@ -438,7 +440,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 for (int r = 0; r < E; ++r) {
                     const int n2 = B::first_pos(tp, r);
                     if constexpr (B::LIFT) {  // the exact inverse of the PF_TW rotations below
-                        const Tw lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
+                        const Lf lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
                         v[r] = lift(lift(cscale(v[r], lo.z * hi.z), -hi.x, -hi.y), -lo.x, -lo.y);
                     } else {
                         v[r] = cmulc(cmulc(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
@@ -474,15 +476,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 // H = P[fbase & 63] * Q[fbase >> 6] * R[r] * h3[r][tp]; k2 >= L/2
                 // (k2s = k2 - L) is decided by the compile-time part of the
                 // frequency, so 0 <= fbase < L/2
-                const Tw *h3 = static_cast<const Tw *>(a.pr.h3);
+                const Lf *h3 = static_cast<const Lf *>(a.pr.h3);
                 if constexpr (B::LIFT) {
                     // three rotations: the thread's P Q (FP64 product), R[r], h3
                     const double2 *chd = reinterpret_cast<const double2 *>(chp);
-                    const Tw tl = lift_of(cmul(chd[fbase & 63], chd[64 + (fbase >> 6) + NQ / 2]));
+                    const Lf tl = lift_of(cmul(chd[fbase & 63], chd[64 + (fbase >> 6) + NQ / 2]));
 #pragma unroll
                     for (int r = 0; r < E; ++r) {
                         const int k2 = fbase | B::freq_off(r);
-                        const Tw rr = chp[64 + NQ + r], g = __ldg(h3 + r * B::T + tp);
+                        const Lf rr = chp[64 + NQ + r], g = __ldg(h3 + r * B::T + tp);
                         Cx x = cscale(v[r], tl.z * rr.z * g.z);
                         x = lift(lift(lift(x, tl.x, tl.y), rr.x, rr.y), g.x, g.y);
                         v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : x;
@@ -527,7 +529,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 for (int r = 0; r < E; ++r) {
                     const int n2 = B::first_pos(tp, r);
                     if constexpr (B::LIFT) {
-                        const Tw lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
+                        const Lf lo = vec[n2 & 63], hi = vec[64 + (n2 >> 6)];
                         v[r] = lift(lift(cscale(v[r], lo.z * hi.z), lo.x, lo.y), hi.x, hi.y);
                     } else {
                         v[r] = cmul(cmul(v[r], vec[n2 & 63]), vec[64 + (n2 >> 6)]);
@@ -563,10 +565,11 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
     // complex64 applies both parts as rotations by lifting (register parts
     // stored in the lifting form).
     using Tw = typename B::Tw;
+    using Lf = typename LiftT<Real>::T;
     using CT = ColTab<B::T>;
     constexpr int LX = CT::LX, NX = 1 << LX, NXY = NX + (1 << CT::LY);
     constexpr int XP = CT::XP, YP = CT::YP, EP = E + 1;
-    constexpr size_t PAR = CT::template parity_bytes<C, E, int(sizeof(Tw))>();
+    constexpr size_t PAR = CT::template parity_bytes<C, E, int(sizeof(Lf))>();
     extern __shared__ __align__(16) unsigned char smraw[];
     const int t = threadIdx.x;
     const int c = t % C;
@@ -592,7 +595,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         // factor tables, double-buffered by tile parity
         double2 *tx = reinterpret_cast<double2 *>(tab0 + parity * PAR);
         double2 *ty = tx + C * XP;
-        Tw *vec = reinterpret_cast<Tw *>(ty + C * YP);
+        Lf *vec = reinterpret_cast<Lf *>(ty + C * YP);
         const int64_t batch = tile >> log_tb;
         const int64_t col0 = (tile & ((int64_t(1) << log_tb) - 1)) * C;  // column within the batch
         const int64_t col = col0 + c;
@@ -620,12 +623,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
             for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
             if (flags & PF_TWI) {
                 __syncthreads();  // this tile's factor table is complete
-                const Tw *vc = vec + c * EP;
+                const Lf *vc = vec + c * EP;
                 const double2 w64 = cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]);
                 const Real s = Real(a.tw_scale);  // a power of two: exact
                 if constexpr (B::LIFT) {
                     // the exact inverse of the PF_TW rotations (register part first)
-                    const Tw wt = lift_of(w64);
+                    const Lf wt = lift_of(w64);
 #pragma unroll
                     for (int r = 0; r < E; ++r)
                         v[r] = lift(lift(cscale(v[r], wt.z * vc[r].z * s), -vc[r].x, -vc[r].y), -wt.x, -wt.y);
@@ -646,10 +649,10 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_FWD) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
-                const Tw *vc = vec + c * EP;
+                const Lf *vc = vec + c * EP;
                 const double2 w64 = cmul(tx[c * XP + (tp & (NX - 1))], ty[c * YP + (tp >> LX)]);
                 if constexpr (B::LIFT) {
-                    const Tw wt = lift_of(w64);
+                    const Lf wt = lift_of(w64);
 #pragma unroll
                     for (int r = 0; r < E; ++r)
                         v[r] = lift(lift(cscale(v[r], wt.z * vc[r].z), wt.x, wt.y), vc[r].x, vc[r].y);
@@ -673,7 +676,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 // Block<Real, LOG_L2, 1, E>, stored at r * T + tp ({cos, sin} for complex128,
 // the lifting form for complex64).
 template <typename Real, int LOG_L2, int E>
-__global__ void chirp_table_kernel(typename TwT<Real>::T *__restrict__ out, double g3_hi, double g3_lo) {
+__global__ void chirp_table_kernel(typename LiftT<Real>::T *__restrict__ out, double g3_hi, double g3_lo) {
     using B = Block<Real, LOG_L2, 1, E>;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= B::L) return;
@@ -708,7 +711,7 @@ template <int L, int E> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L
 template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
     auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
-    const size_t smem = B::SMEM + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * sizeof(typename B::Tw);
+    const size_t smem = (B::SMEM + 15) / 16 * 16 + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * 16;
     static cudaError_t attr = prep(k, smem);
     if (attr != cudaSuccess) return attr;
     static int64_t cap = resident_ctas(k, B::NT, smem);
@@ -739,7 +742,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
     auto k = col_pass_kernel<Real, LG, C, E>;
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
-    const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, int(sizeof(typename B::Tw))>();
+    const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, 16>();
     static cudaError_t attr = prep(k, tab);
     if (attr != cudaSuccess) return attr;
     static int64_t cap_tab = resident_ctas(k, B::NT, tab);
@@ -755,7 +758,7 @@ template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const
 
 template <typename Real, int LG, int E> static cudaError_t chirp_impl(void *out, double hi, double lo, cudaStream_t s) {
     chirp_table_kernel<Real, LG, E><<<((1 << LG) + 255) / 256, 256, 0, s>>>(
-        static_cast<typename TwT<Real>::T *>(out), hi, lo);
+        static_cast<typename LiftT<Real>::T *>(out), hi, lo);
     count_launch();
     return cudaGetLastError();
 }

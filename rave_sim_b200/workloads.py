@@ -181,15 +181,18 @@ def cracked_cylinder(rows=200, cols=4000, psz=10e-6, psx=0.5e-6, diameter=2e-3, 
 
 
 def thick_sample(n=1 << 26, dx=50e-9, dtype="c8", nr_steps=10, phase_steps=8, rows=200, cols=4000,
-                 psz=10e-6, psx=0.5e-6, gap=1e-3, seed=4):
+                 psz=10e-6, psx=0.5e-6, gap=1e-3, seed=4, diameter=2e-3, axis_range=(1e-6, 20e-6),
+                 detector_size=2.048e-3, pixel_size=1e-6):
     """Benchmark config 4: the interferometer with a ``sample`` element (the
     cracked cylinder of ``cracked_cylinder``) starting ``gap`` after the G1
     exit. Returns (case, grids) with the grid under element index 2; the
-    deltabeta table of an energy is ``db_table_sample``."""
-    case = talbot_lau(n=n, dx=dx, dtype=dtype, nr_steps=nr_steps, phase_steps=phase_steps)
+    deltabeta table of an energy is ``db_table_sample``. The phantom and
+    detector arguments scale the setup down for parity tests."""
+    case = talbot_lau(n=n, dx=dx, dtype=dtype, nr_steps=nr_steps, phase_steps=phase_steps,
+                      detector_size=detector_size, pixel_size=pixel_size)
     g1 = case["elements"][1]
     z0 = g1["z_start"] + g1["thickness"] + gap
-    grid = cracked_cylinder(rows, cols, psz, psx, seed=seed)
+    grid = cracked_cylinder(rows, cols, psz, psx, diameter=diameter, axis_range=axis_range, seed=seed)
     sample = {"type": "sample", "z_start": z0, "pixel_size_x": psx, "pixel_size_z": psz,
               "grid_path": "cracked_cylinder.npy", "materials": [AL], "x_positions": [0.0]}
     case["elements"].insert(2, sample)
