@@ -89,10 +89,14 @@ rsw_status rsw_fft_inverse(rsw_plan plan, const void *d_in, void *d_out, void *s
  * image (held by every GPU that loads the library until exit), so n is
  * limited to RSW_NOALLOC_MAX_N samples; larger n returns RSW_ERR_INVALID.
  * The first call on each device (with that device current) looks up the
- * array's device address; make that call before any stream capture. All
- * calls share the array and it keeps the last call's contents (tables are
- * rebuilt when n or dtype changes); calls that overlap on the GPU race and
- * must be serialised by the caller. in == out is allowed. */
+ * array's device address, and the first call for each n and dtype on a
+ * device builds that length's twiddle tables in its own part of the array
+ * (never rebuilt afterwards); make those calls before any stream capture: a
+ * first call for an n and dtype made while the stream is capturing returns
+ * RSW_ERR_INVALID. A CUDA error left pending by earlier work is reported
+ * (RSW_ERR_CUDA) and not cleared. All calls share the array's intermediate
+ * spectrum and it keeps the last call's contents; calls that overlap on the
+ * GPU race and must be serialised by the caller. in == out is allowed. */
 #define RSW_NOALLOC_MAX_N 65536
 rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int64_t n, int dtype, void *stream);
 
@@ -265,8 +269,10 @@ rsw_status rsw_sim_accumulator(rsw_sim sim, double **d_acc);
 rsw_status rsw_sim_final_field(rsw_sim sim, void *d_dst, void *stream);
 
 /* Per-kernel-kind device timing of the next rsw_sim_run calls (CUDA events on
- * the run's stream). kind: 0 = row pass, 1 = column pass, 2 = detection,
- * 3 = middle pass (three-level plans, N above the two-level limit).
+ * the run's stream). kind: 0 = row pass, 1 = column pass, 2 = detection (the
+ * last inverse column pass of each phase step, with the |u|^2 binning fused
+ * in; the binning kernel alone for single-level plans), 3 = middle pass
+ * (three-level plans, N above the two-level limit).
  * rsw_sim_timing returns the summed milliseconds and launch counts since
  * enabling; it synchronises. */
 rsw_status rsw_sim_set_timing(rsw_sim sim, int enable);

@@ -28,8 +28,9 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
 ]
 
-SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_kernels.cu", "rsw_noalloc.cu", "rsw_host.cpp"]
-HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh"]
+SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_col_det.cu", "rsw_kernels.cu", "rsw_noalloc.cu",
+           "rsw_host.cpp"]
+HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh", "rsw_stages.h", "rsw_col_dispatch.h"]
 
 
 def nvcc() -> str:

@@ -43,10 +43,13 @@
 // linearly and dominated the complex64 detector error (lifting: growth like
 // the square root of the step count, measured 17x smaller after 200 steps in
 // a float32 model of the forward/inverse pair). Table entries of complex64
-// blocks are {a, b} with the half turn in the lowest mantissa bit of a (a is
-// rounded to the nearest float of that parity: the rotation angle moves by
-// at most one ulp of a, the same in the forward and the inverse pass, and the
-// shears keep determinant 1); complex128 blocks keep {cos, sin}.
+// blocks are {a, b}. Angles beyond a quarter turn (tw_mode, rsw_stages.h)
+// take a fixed quarter turn in the code where the output index q bounds the
+// angle below a half turn, and otherwise a half-turn flag in the lowest
+// mantissa bit of a (a is rounded to the nearest float of that parity: the
+// rotation angle moves by at most one ulp of a, the same in the forward and
+// the inverse pass, and the shears keep determinant 1); complex128 blocks
+// keep {cos, sin}.
 //
 // Shared memory holds the C sequences with one pad element per E (phys(p):
 // the last stage gives consecutive threads positions E apart, which the pad
@@ -329,21 +332,33 @@ struct Block : Radix<LOG_L, E_, direct_max_ls(2 * sizeof(Real), LOG_L)> {
             return cmul(a, b);
         }
     }
-    // complex64: x * W_{RS}^{j q} (INV: x * conj(W)) by lifting; a factored
-    // twiddle is two rotations, undone in reverse order by the inverse
+    // complex64: x * W_{RS}^{j q} (INV: x * conj(W)) by lifting, with the
+    // entry's tw_mode (q is a constant after unrolling): mode 1 adds the fixed
+    // quarter turn, mode 2 the half turn of the entry's flag. A factored
+    // twiddle is two rotations (the low factor is mode 0), undone in reverse
+    // order by the inverse.
+    template <bool INV> __device__ static __forceinline__ Cx rot_mode(Cx x, Tw w, int mode) {
+        if (mode == 2) x = cscale(x, half_turn(w.x));
+        if (INV) {
+            if (mode == 1) x = quarter<1>(x);
+            return lift(x, -w.x, -w.y);
+        }
+        x = lift(x, w.x, w.y);
+        return mode == 1 ? quarter<-1>(x) : x;
+    }
     template <int s, bool INV> __device__ static __forceinline__ Cx twlift(const Tw *tw, int j, int q, Cx x) {
         constexpr int LSS = Rx::ls(s);
+        constexpr int R = 1 << Rx::lr(s);
         const Tw *t = tw + Rx::twoff(s);
+        const int mode = tw_mode(q, R);
         if constexpr (Rx::direct(s)) {
-            const Tw w = t[((q - 1) << LSS) + j];
-            return INV ? rot_inv(x, w) : rot(x, w);
+            return rot_mode<INV>(x, t[((q - 1) << LSS) + j], mode);
         } else {
-            constexpr int R = 1 << Rx::lr(s);
+            static_assert(LSS >= 8, "factored stages have strides >= 256 (low factors below a quarter turn)");
             const Tw a = t[(q - 1) * 64 + (j & 63)];
             const Tw b = t[(R - 1) * 64 + (q - 1) * (1 << (LSS - 6)) + (j >> 6)];
-            x = cscale(x, half_turn2(a.x, b.x));
-            if constexpr (INV) return lift(lift(x, -b.x, -b.y), -a.x, -a.y);
-            else return lift(lift(x, a.x, a.y), b.x, b.y);
+            if constexpr (INV) return lift(rot_mode<true>(x, b, mode), -a.x, -a.y);
+            else return rot_mode<false>(lift(x, a.x, a.y), b, mode);
         }
     }
 

@@ -28,6 +28,7 @@
 namespace rsw {
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s);
+cudaError_t launch_col_detect(const PassArgs &a, bool dbl, int e, cudaStream_t s);
 cudaError_t launch_spec_to_natural(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
                                    cudaStream_t s);
 cudaError_t launch_natural_to_spec(const void *in, void *out, int64_t n, const SpecLevels &v, bool dbl,
@@ -329,22 +330,28 @@ template <typename T> static void push_c(std::vector<T> &v, cplx c) {
 }
 
 // Packed lifting form {a, b} of W_M^m = exp(-2 pi i m / M) for complex64
-// block tables (rotation by three shears, rsw_block_fft.cuh): m is reduced to
-// (-M/2, M/2]; beyond a quarter turn a half turn is taken out, so that the
-// remaining angle t = -2 pi m' / M has |t| <= pi/2; a = -tan(t/2), b = sin(t).
-// The half turn is the lowest mantissa bit of a: a is rounded to the nearest
-// float whose low bit is the half-turn flag.
-static void push_lift(std::vector<float> &v, int64_t m, int64_t M) {
+// block tables (rotation by three shears, rsw_block_fft.cuh), for the entry's
+// tw_mode (rsw_stages.h): mode 0 rotates by the angle itself (below a quarter
+// turn), mode 1 by the angle + pi/2 (the kernel adds the quarter turn); mode
+// 2 reduces m to (-M/2, M/2] and beyond a quarter turn takes out a half
+// turn, carried in the lowest mantissa bit of a (a is rounded to the nearest
+// float whose low bit is the flag). Then t = -2 pi m' / M has |t| <= pi/2,
+// a = -tan(t/2), b = sin(t).
+static void push_lift(std::vector<float> &v, int64_t m, int64_t M, int mode) {
     m %= M;
     if (m < 0) m += M;
-    if (m > M / 2) m -= M;
     unsigned flip = 0;
-    if (4 * m > M) {
-        m -= M / 2;
-        flip = 1;
-    } else if (4 * m < -M) {
-        m += M / 2;
-        flip = 1;
+    if (mode == 1) {
+        m -= M / 4;
+    } else if (mode == 2) {
+        if (m > M / 2) m -= M;
+        if (4 * m > M) {
+            m -= M / 2;
+            flip = 1;
+        } else if (4 * m < -M) {
+            m += M / 2;
+            flip = 1;
+        }
     }
     const long double pi = 3.14159265358979323846264338327950288L;
     const long double t = -2.0L * pi * (long double)m / (long double)M;
@@ -352,7 +359,7 @@ static void push_lift(std::vector<float> &v, int64_t m, int64_t M) {
     float af = float(a);
     uint32_t bits;
     std::memcpy(&bits, &af, 4);
-    if ((bits & 1u) != flip) af = std::nextafter(af, (long double)af < a ? HUGE_VALF : -HUGE_VALF);
+    if (mode == 2 && (bits & 1u) != flip) af = std::nextafter(af, (long double)af < a ? HUGE_VALF : -HUGE_VALF);
     v.push_back(af);
     v.push_back(float(sinl(t)));
 }
@@ -370,13 +377,13 @@ template <typename T> static std::vector<T> block_twiddles(int log_l, int rb) {
             for (int64_t k = 0; k < stage_tw_entries(log_l, s, max_ls, rb); ++k) {
                 int64_t m, mod;
                 stage_tw_entry(log_l, s, max_ls, rb, k, &m, &mod);
-                if constexpr (lift) push_lift(v, m, mod);
+                if constexpr (lift) push_lift(v, m, mod, stage_tw_mode(log_l, s, max_ls, rb, k));
                 else push_c(v, twiddle(m, mod));
             }
         }
     }
     if (v.empty()) {
-        if constexpr (lift) push_lift(v, 0, 1);
+        if constexpr (lift) push_lift(v, 0, 1, 0);
         else push_c(v, cplx(1, 0));
     }
     return v;
@@ -1229,6 +1236,7 @@ struct rsw_sim_s {
     DetectorGeom geom;
     DevBuf bounds, cosv, rv;
     DevBuf acc, comp;
+    DevBuf dsum;  // fused detection: n_pix raw sums, then the CTA counter (kept zero between passes)
     DevBuf buf[2];
     DevBuf mat_db, mat_fac;  // per-run sample material tables
     std::vector<std::unique_ptr<DevBuf>> h3_pool;  // chirp tables, one per distinct dz of a run
@@ -1462,6 +1470,48 @@ struct Runner {
         return RSW_OK;
     }
 
+    // The end of a phase step: the field's last inverse column pass with the
+    // detector binning fused in (the field is written only when `keep`, for
+    // the final field of a run); the plain inverse and the binning kernel
+    // where the field is not in the multi-level "mid" representation.
+    rsw_status finish_phase(int64_t phase, double weight, bool keep) {
+        const int64_t np = S->geom.n_pix;
+        if (!(mid && P->log_n1 > 0 && np > 0)) {
+            CHECK(finalize());
+            return detect(phase, weight);
+        }
+        const int dst = target();
+        PassArgs a = base_args(P);
+        a.in = S->buf[cur].p;
+        a.out = S->buf[dst].p;
+        a.flags = col_inv(P) | (keep ? 0 : PF_NOSTORE);
+        DetectArgs &d = a.det;
+        d.bounds = (const int64_t *)S->bounds.p;
+        d.cosv = (const double *)S->cosv.p;
+        d.rv = (const double *)S->rv.p;
+        d.n_pix = np;
+        d.lo = S->geom.bounds[0];
+        d.hi = S->geom.bounds[size_t(np)];
+        d.inv_w = d.hi > d.lo ? double(np) / double(d.hi - d.lo) : 0.0;
+        d.dx = S->d.dx;
+        d.psy = S->d.pixel_size_y;
+        d.weight = weight;
+        d.sum = (double *)S->dsum.p;
+        d.count = (unsigned *)((double *)S->dsum.p + np);
+        d.acc = (double *)S->acc.p + phase * np;
+        d.comp = (double *)S->comp.p + phase * np;
+        TimingLog::Rec r{};
+        if (S->tl.enabled) S->tl.begin(2, st, r);
+        cudaError_t e = launch_col_detect(a, P->dbl(), P->col_e, st);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "detection pass (2^%d): %s", a.log_n1, cudaGetErrorString(e));
+        if (S->tl.enabled) S->tl.end(r, st);
+        if (keep) {
+            cur = dst;
+            mid = false;
+        }
+        return RSW_OK;
+    }
+
     rsw_status detect(int64_t phase, double weight) {
         TimingLog::Rec r{};
         if (S->tl.enabled) S->tl.begin(2, st, r);
@@ -1624,6 +1674,9 @@ rsw_status rsw_sim_create(rsw_sim *out, const rsw_sim_desc *desc) {
     CHECK(S->comp.alloc(std::max<size_t>(nacc, 1) * sizeof(double)));
     CU(cudaMemset(S->acc.p, 0, nacc * sizeof(double)));
     CU(cudaMemset(S->comp.p, 0, nacc * sizeof(double)));
+    const size_t dsum_bytes = size_t(S->geom.n_pix) * sizeof(double) + 16;
+    CHECK(S->dsum.alloc(dsum_bytes));
+    CU(cudaMemset(S->dsum.p, 0, dsum_bytes));
     const size_t fb = size_t(desc->n) * S->plan->elem();
     CHECK(S->buf[0].alloc(fb));
     if (S->nr_phase_steps > 1) CHECK(S->buf[1].alloc(fb));
@@ -1844,8 +1897,7 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
         z = e.z_start + s.els[i].total_thickness();
     }
     if (z < s.d.z_detector - z_tol) CHECK(R.gap(s.d.z_detector - z, cutoff, z));
-    CHECK(R.finalize());
-    CHECK(R.detect(0, run->weight));
+    CHECK(R.finish_phase(0, run->weight, s.nr_phase_steps == 1));
     R.hist_on = false;  // phase steps from the snapshot record no history (big-wave/wavesim.py:234-237)
 
     // ---- remaining phase steps from the snapshot (big-wave/wavesim.py:238-296)
@@ -1864,8 +1916,7 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
             z = e.z_start + s.els[i].total_thickness();
         }
         if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, cutoff));
-        CHECK(R.finalize());
-        CHECK(R.detect(step, run->weight));
+        CHECK(R.finish_phase(step, run->weight, step == s.nr_phase_steps - 1));
     }
     s.last_field = R.cur;
     return RSW_OK;

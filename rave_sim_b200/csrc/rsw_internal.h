@@ -68,6 +68,25 @@ enum PassFlags : int {
     PF_SPEC_IN = 64,  // row: input is a spectrum (digit-reversed layout), start with the inverse
     PF_TWI = 128,     // column: before the inverse, conj(W_M^(n2 k1)) * tw_scale
     PF_TWF = 256,     // row: before the forward, W_M^(n2 tw_k) (the conjugate of PF_TW's factor)
+    PF_NOSTORE = 512, // column detection pass: bin the field only, do not write it
+};
+
+// Detector binning fused into the last inverse column pass of a phase step
+// (square_and_downsample, big-wave/propagation.py:279-320). Pixel j holds the
+// samples [bounds[j], bounds[j+1]) (np.histogram bins, built on the host);
+// the pass adds |u|^2 of its samples into sum[j] (FP64, zero between passes),
+// and the CTA that finishes last adds weight * (((sum cos_j) dx) psy) / r_j
+// into acc/comp (Kahan) and zeroes sum and count again.
+struct DetectArgs {
+    const int64_t *bounds;   // n_pix + 1
+    const double *cosv, *rv; // per pixel
+    int64_t n_pix;
+    int64_t lo, hi;          // bounds[0], bounds[n_pix]: the detector's sample range
+    double inv_w;            // n_pix / (hi - lo): first guess of a sample's pixel
+    double dx, psy, weight;
+    double *sum;             // n_pix raw sums
+    unsigned *count;         // CTAs done
+    double *acc, *comp;      // the phase step's accumulator row
 };
 
 // Arguments of one pass. N = N1 * N2 samples; three-level plans split the
@@ -95,6 +114,7 @@ struct PassArgs {
     double tw_scale;      // factor of the conjugate twiddles (1/N at the last inverse level)
     TransArgs tr;
     PropArgs pr;
+    DetectArgs det;
 };
 
 // Level structure of the internal spectrum layout (log2 lengths and digit

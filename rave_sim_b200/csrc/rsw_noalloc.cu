@@ -10,19 +10,25 @@
 // buffer per plan); this entry point does not.
 //
 // Its scratch is the file-scope array g_noalloc_scratch below (1.5 MiB): the
-// intermediate spectrum of up to RSW_NOALLOC_MAX_N samples plus the twiddle
-// tables of the current length. Every GPU that loads the library holds the
-// array until the process exits. Host code never dereferences the symbol: on
-// the first call on each device (with that device current) the device address
-// is taken once with cudaGetSymbolAddress and passed to the kernels.
+// intermediate spectrum of up to RSW_NOALLOC_MAX_N samples, then one slot of
+// twiddle tables for every length (2^4 .. 2^16) and dtype, 258 KiB in all.
+// Every GPU that loads the library holds the array until the process exits.
+// Host code never dereferences the symbol: on the first call on each device
+// (with that device current) the device address is taken with
+// cudaGetSymbolAddress and passed to the kernels; it is taken again when the
+// device's context changes (after a cudaDeviceReset).
 //
-// All calls share the array and it keeps the last call's contents: the
-// tables are rebuilt (by a small kernel on the caller's stream) whenever the
-// length or dtype differs from the previous call on that device, and every
-// scratch sample a call reads was written earlier in the same call, so
+// The first call for a length and dtype on a device builds that slot's tables
+// with a small kernel on the caller's stream; later calls reuse the slot, which
+// is never rebuilt, so a call for another length cannot change the tables of
+// this one. A first call made while `stream` is capturing a graph is refused
+// (RSW_ERR_INVALID), since its table build would only run at a replay. All
+// calls share the spectrum and it keeps the last call's contents; every
+// spectrum sample a call reads was written earlier in the same call, so
 // nothing needs clearing. Calls whose work overlaps on the GPU (different
 // streams without ordering, or several host threads) race on the array and
-// must be serialised by the caller.
+// must be serialised by the caller, including a call that overlaps the first
+// call for its length and dtype.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -45,30 +51,67 @@ using namespace rsw;
 namespace {
 
 constexpr int64_t MAX_N = RSW_NOALLOC_MAX_N;
+constexpr int LOG_MIN = 4, LOG_MAX = 16;
+constexpr int KEYS = 2 * (LOG_MAX - LOG_MIN + 1);     // (length, dtype) pairs
+constexpr size_t ARRAY_BYTES = 1536 * 1024;
 constexpr size_t SPEC_BYTES = size_t(MAX_N) * 16;  // intermediate spectrum, complex128 worst case
-constexpr size_t BLOCK_TW_ENTRIES = 8192;           // per level, >= the block twiddles of 2^8 (both dtypes)
-constexpr size_t TW4_ENTRIES = 256;                 // 2^ceil(16/2)
-constexpr size_t OFF_TWROW = SPEC_BYTES;
-constexpr size_t OFF_TWCOL = OFF_TWROW + BLOCK_TW_ENTRIES * 16;
-constexpr size_t OFF_TW4LO = OFF_TWCOL + BLOCK_TW_ENTRIES * 16;
-constexpr size_t OFF_TW4HI = OFF_TW4LO + TW4_ENTRIES * 16;
-constexpr size_t SCRATCH_BYTES = OFF_TW4HI + TW4_ENTRIES * 16;
-static_assert(SCRATCH_BYTES <= 1536 * 1024, "scratch layout exceeds the array");
+
+// The level split of the plans: one level up to 2^13 (c128) / 2^14 (c64),
+// then two levels.
+constexpr int split_n1(int log_n, bool dbl) { return log_n > (dbl ? 13 : 14) ? log_n / 2 : 0; }
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+// bytes of the block twiddles of a length-2^log_l block (16 samples per
+// thread, radix-16 stages; 16-byte entries for complex128, 8 for complex64)
+constexpr size_t block_tw_bytes(int log_l, bool dbl) {
+    const int eb = dbl ? 16 : 8;
+    const int max_ls = direct_max_ls(eb, log_l);
+    int64_t n = 0;
+    for (int s = 0; s < stage_count(log_l) - 1; ++s) n += stage_tw_entries(log_l, s, max_ls);
+    return size_t(n > 0 ? n : 1) * size_t(eb);
+}
+// The table slot of one (length, dtype): block twiddles of the row and
+// column levels, then the FP64 four-step tables lo[2^h], hi[2^(log_n - h)].
+struct Slot {
+    size_t tw_row, tw_col, tw4_lo, tw4_hi, end;
+};
+constexpr Slot slot_at(size_t base, int log_n, bool dbl) {
+    const int l1 = split_n1(log_n, dbl), l2 = log_n - l1, h = (log_n + 1) / 2;
+    Slot s{};
+    s.tw_row = base;
+    s.tw_col = align256(s.tw_row + block_tw_bytes(l2, dbl));
+    s.tw4_lo = align256(s.tw_col + (l1 > 0 ? block_tw_bytes(l1, dbl) : 0));
+    s.tw4_hi = align256(s.tw4_lo + (l1 > 0 ? (size_t(1) << h) * 16 : 0));
+    s.end = align256(s.tw4_hi + (l1 > 0 ? (size_t(1) << (log_n - h)) * 16 : 0));
+    return s;
+}
+constexpr int key_of(int log_n, int dtype) { return (log_n - LOG_MIN) * 2 + dtype; }
+// slots in key order after the spectrum
+constexpr Slot slot_of(int key) {
+    size_t base = SPEC_BYTES;
+    for (int k = 0;; ++k) {
+        const Slot s = slot_at(base, LOG_MIN + k / 2, (k % 2) == RSW_C128);
+        if (k == key) return s;
+        base = s.end;
+    }
+}
+static_assert(slot_of(KEYS - 1).end <= ARRAY_BYTES, "table slots exceed the array");
 
 }  // namespace
 
 // The scratch array of rsw_fft_forward_noalloc (see the file comment).
-static __device__ __align__(256) unsigned char g_noalloc_scratch[1536 * 1024];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[ARRAY_BYTES];
 
 namespace {
 
 // Block twiddles of a block of length 2^log_l into `out` in the layout of
 // the block FFT (rsw_stages.h): W_M^m = exp(-2 pi i m / M) as {cos, sin}
 // (FP64) from sincospi of an exact argument, or for complex64 the packed
-// lifting form {a, b}: m reduced to (-M/2, M/2], a half turn taken out beyond
-// a quarter turn, a = -tan(t/2), b = sin(t) of the remaining angle
-// t = -2 pi m' / M, and a rounded to the nearest float whose lowest mantissa
-// bit is the half-turn flag (the rule of the host-built tables).
+// lifting form {a, b} by the entry's tw_mode (the rule of the host-built
+// tables): mode 1 takes out a quarter turn, mode 2 reduces m to
+// (-M/2, M/2] and takes out a half turn beyond a quarter turn, then
+// a = -tan(t/2), b = sin(t) of the remaining angle t = -2 pi m' / M; in mode
+// 2 a is rounded to the nearest float whose lowest mantissa bit is the
+// half-turn flag.
 template <typename T>
 __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     int off = 0;
@@ -84,21 +127,27 @@ __device__ void block_tables(T *out, int log_l, int idx, int stride) {
                 out[2 * (off + k)] = T(cs);
                 out[2 * (off + k) + 1] = T(sn);
             } else {
+                const int mode = stage_tw_mode(log_l, s, max_ls, 4, k);
                 m %= mod;
-                if (m > mod / 2) m -= mod;
                 unsigned flip = 0;
-                if (4 * m > mod) {
-                    m -= mod / 2;
-                    flip = 1;
-                } else if (4 * m < -mod) {
-                    m += mod / 2;
-                    flip = 1;
+                if (mode == 1) {
+                    m -= mod / 4;
+                } else if (mode == 2) {
+                    if (m > mod / 2) m -= mod;
+                    if (4 * m > mod) {
+                        m -= mod / 2;
+                        flip = 1;
+                    } else if (4 * m < -mod) {
+                        m += mod / 2;
+                        flip = 1;
+                    }
                 }
                 double sh, ch;
                 sincospi(double(m) / double(mod), &sh, &ch);  // angle -t/2
                 const double a = sh / ch;                       // -tan(t/2)
                 float af = float(a);
-                if ((__float_as_uint(af) & 1u) != flip) af = nextafterf(af, double(af) < a ? HUGE_VALF : -HUGE_VALF);
+                if (mode == 2 && (__float_as_uint(af) & 1u) != flip)
+                    af = nextafterf(af, double(af) < a ? HUGE_VALF : -HUGE_VALF);
                 out[2 * (off + k)] = af;
                 out[2 * (off + k) + 1] = T(-sinpi(2.0 * double(m) / double(mod)));  // sin(t)
             }
@@ -107,34 +156,53 @@ __device__ void block_tables(T *out, int log_l, int idx, int stride) {
     }
 }
 
-__global__ void noalloc_tables_kernel(unsigned char *scratch, int log_n, int log_n1, int log_n2, int dbl) {
+__global__ void noalloc_tables_kernel(unsigned char *scratch, Slot slot, int log_n, int log_n1, int log_n2, int dbl) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     const int stride = gridDim.x * blockDim.x;
     if (dbl) {
-        block_tables(reinterpret_cast<double *>(scratch + OFF_TWROW), log_n2, idx, stride);
-        if (log_n1 > 0) block_tables(reinterpret_cast<double *>(scratch + OFF_TWCOL), log_n1, idx, stride);
+        block_tables(reinterpret_cast<double *>(scratch + slot.tw_row), log_n2, idx, stride);
+        if (log_n1 > 0) block_tables(reinterpret_cast<double *>(scratch + slot.tw_col), log_n1, idx, stride);
     } else {
-        block_tables(reinterpret_cast<float *>(scratch + OFF_TWROW), log_n2, idx, stride);
-        if (log_n1 > 0) block_tables(reinterpret_cast<float *>(scratch + OFF_TWCOL), log_n1, idx, stride);
+        block_tables(reinterpret_cast<float *>(scratch + slot.tw_row), log_n2, idx, stride);
+        if (log_n1 > 0) block_tables(reinterpret_cast<float *>(scratch + slot.tw_col), log_n1, idx, stride);
     }
     if (log_n1 > 0) {  // four-step tables (FP64): lo[a] = W_N^a, hi[b] = W_N^(b 2^h)
         const int h = (log_n + 1) / 2;
         const double n = double(int64_t(1) << log_n);
-        double *lo = reinterpret_cast<double *>(scratch + OFF_TW4LO);
-        double *hi = reinterpret_cast<double *>(scratch + OFF_TW4HI);
+        double *lo = reinterpret_cast<double *>(scratch + slot.tw4_lo);
+        double *hi = reinterpret_cast<double *>(scratch + slot.tw4_hi);
         for (int a = idx; a < (1 << h); a += stride) sincospi(-2.0 * a / n, &lo[2 * a + 1], &lo[2 * a]);
         for (int b = idx; b < (1 << (log_n - h)); b += stride)
             sincospi(-2.0 * double(int64_t(b) << h) / n, &hi[2 * b + 1], &hi[2 * b]);
     }
 }
 
+// Per device: the context the state belongs to (a device reset gives a new
+// one), the array's device address in it, and the slots built there.
 struct DeviceState {
-    void *ptr = nullptr;  // device address of g_noalloc_scratch
-    int key = -1;         // log_n * 2 + dtype of the tables currently in the array
+    void *ctx = nullptr;
+    unsigned char *ptr = nullptr;
+    bool built[KEYS] = {};
 };
 constexpr int MAX_DEVICES = 64;
 DeviceState g_state[MAX_DEVICES];
 std::mutex g_mutex;
+
+// the current context (driver cuCtxGetCurrent through the runtime's entry point)
+void *current_context() {
+    using Fn = int (*)(void **);
+    static Fn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<Fn>(p);
+    }();
+    void *ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 rsw_status fail_na(rsw_status st, const char *msg) {
     char buf[256];
@@ -151,45 +219,57 @@ extern "C" rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int
     if (n > MAX_N) return fail_na(RSW_ERR_INVALID, "n exceeds the no-allocation limit of 65536 samples");
     int log_n = 0;
     while ((int64_t(1) << log_n) < n) ++log_n;
-    // the same level split as the plans: one level up to 2^13 (c128) / 2^14 (c64)
     const bool dbl = dtype == RSW_C128;
-    const int row_max = dbl ? 13 : 14;
-    int log_n1 = 0, log_n2 = log_n;
-    if (log_n > row_max) {
-        log_n1 = log_n / 2;
-        log_n2 = log_n - log_n1;
-    }
+    const int log_n1 = split_n1(log_n, dbl), log_n2 = log_n - log_n1;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
         return fail_na(RSW_ERR_CUDA, "no current device");
+    // an error left by earlier work is not this call's to report or clear
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "a CUDA error from earlier work is pending: %s", cudaGetErrorString(pending));
+        return fail_na(RSW_ERR_CUDA, msg);
+    }
+    const int key = key_of(log_n, dtype);
+    const Slot slot = slot_of(key);
     unsigned char *scratch;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
         DeviceState &st = g_state[dev];
-        if (!st.ptr) {
+        void *ctx = current_context();
+        if (!st.ptr || ctx != st.ctx) {
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
-            st.ptr = p;
+            st = DeviceState{};
+            st.ctx = ctx;
+            st.ptr = static_cast<unsigned char *>(p);
         }
-        scratch = static_cast<unsigned char *>(st.ptr);
-        const int key = log_n * 2 + dtype;
-        if (st.key != key) {
-            noalloc_tables_kernel<<<16, 256, 0, s>>>(scratch, log_n, log_n1, log_n2, dbl ? 1 : 0);
+        scratch = st.ptr;
+        if (!st.built[key]) {
+            cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+            const cudaError_t ce = cudaStreamIsCapturing(s, &cap);
+            if (ce != cudaSuccess) return fail_na(RSW_ERR_CUDA, cudaGetErrorString(ce));
+            if (cap != cudaStreamCaptureStatusNone)
+                return fail_na(RSW_ERR_INVALID,
+                               "the first call for this length and dtype on a device builds its tables and "
+                               "cannot be made while the stream is capturing");
+            noalloc_tables_kernel<<<16, 256, 0, s>>>(scratch, slot, log_n, log_n1, log_n2, dbl ? 1 : 0);
             const cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return fail_na(RSW_ERR_CUDA, cudaGetErrorString(e));
-            st.key = key;
+            st.built[key] = true;
         }
     }
     PassArgs a{};
     a.n = n;
     a.log_n1 = log_n1;
     a.log_n2 = log_n2;
-    a.tw_row = scratch + OFF_TWROW;
-    a.tw_col = scratch + OFF_TWCOL;
-    a.tw4_lo = scratch + OFF_TW4LO;
-    a.tw4_hi = scratch + OFF_TW4HI;
+    a.tw_row = scratch + slot.tw_row;
+    a.tw_col = scratch + slot.tw_col;
+    a.tw4_lo = scratch + slot.tw4_lo;
+    a.tw4_hi = scratch + slot.tw4_hi;
     a.tw4_shift = (log_n + 1) / 2;
     a.tw_log = log_n;
     a.rb_n1 = 4;

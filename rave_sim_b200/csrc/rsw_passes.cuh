@@ -28,6 +28,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "rsw_block_fft.cuh"
 #include "rsw_internal.h"
 
@@ -550,11 +552,93 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
     }
 }
 
-template <typename Real, int LOG_L1, int C, int E>
+// ------------------------------------------------------- fused detection
+// Pixel of sample n in [d.lo, d.hi): the linear guess is off by at most a
+// sample or two for np.histogram bins on a uniform grid; bounded steps, then
+// a bisection if they did not bracket it.
+__device__ __forceinline__ int64_t pixel_of(const DetectArgs &d, int64_t n) {
+    int64_t j = int64_t(double(n - d.lo) * d.inv_w);
+    j = j < 0 ? 0 : (j >= d.n_pix ? d.n_pix - 1 : j);
+    for (int it = 0; it < 4 && n < __ldg(d.bounds + j); ++it) --j;
+    for (int it = 0; it < 4 && n >= __ldg(d.bounds + j + 1); ++it) ++j;
+    if (n < __ldg(d.bounds + j) || n >= __ldg(d.bounds + j + 1)) {
+        int64_t a = 0, b = d.n_pix - 1;  // last j with bounds[j] <= n
+        while (a < b) {
+            const int64_t m = (a + b + 1) / 2;
+            if (__ldg(d.bounds + m) <= n) a = m; else b = m - 1;
+        }
+        j = a;
+    }
+    return j;
+}
+
+// |u|^2 of a thread's samples (column col, rows first_pos(tp, r)) into
+// d.sum by pixel. The C lanes of one tp hold adjacent columns of the same
+// rows; a group of G = min(C, 32) lanes whose samples share a pixel adds its
+// group sum with one atomic, otherwise each lane adds its own.
+template <typename B, typename Cx>
+__device__ __forceinline__ void detect_bin(const DetectArgs &d, int64_t base, int64_t col, int tp, const Cx *v,
+                                           int log_n2) {
+    constexpr int C = B::NT / B::T, G = C < 32 ? C : 32;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~unsigned(G - 1));
+#pragma unroll
+    for (int r = 0; r < B::E; ++r) {
+        const int64_t n = base + (int64_t(B::first_pos(tp, r)) << log_n2) + col;
+        const bool in = n >= d.lo && n < d.hi;
+        if (!__any_sync(0xffffffffu, in)) continue;
+        int64_t j = -1;
+        double s = 0.0;
+        if (in) {
+            j = pixel_of(d, n);
+            const double re = double(v[r].x), im = double(v[r].y);
+            s = re * re + im * im;
+        }
+        const int64_t lead = __shfl_sync(0xffffffffu, j, 0, G);
+        const bool uniform = (__ballot_sync(0xffffffffu, j == lead) & gmask) == gmask;
+        double g = s;
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o, G);
+        if (uniform) {
+            if ((lane & unsigned(G - 1)) == 0 && lead >= 0) atomicAdd(d.sum + lead, g);
+        } else if (j >= 0) {
+            atomicAdd(d.sum + j, s);
+        }
+    }
+}
+
+// End of a detection pass: the CTA that finishes last turns the sums into
+// the pixel values of square_and_downsample, (((sum cos_j) dx) psy) / r_j,
+// adds weight * value into the accumulator with Kahan compensation, and
+// zeroes the sums and the count for the next pass.
+__device__ __forceinline__ void detect_finish(const DetectArgs &d) {
+    __shared__ int last;
+    __threadfence();  // this thread's atomics before the count
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(d.count, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int64_t j = threadIdx.x; j < d.n_pix; j += blockDim.x) {
+        const double s = __ldcg(d.sum + j);
+        const double val = (((s * __ldg(d.cosv + j)) * d.dx) * d.psy) / __ldg(d.rv + j);
+        const double y = __dsub_rn(__dmul_rn(d.weight, val), d.comp[j]);
+        const double t = __dadd_rn(d.acc[j], y);
+        d.comp[j] = __dsub_rn(__dsub_rn(t, d.acc[j]), y);
+        d.acc[j] = t;
+        d.sum[j] = 0.0;
+    }
+    if (threadIdx.x == 0) *d.count = 0u;
+}
+
+// DET: the detection variant, for the inverse-only pass that ends a phase
+// step: each CTA takes a contiguous range of tiles (adjacent columns), bins
+// |u|^2 after the inverse transform (detect_bin) and stores the field unless
+// PF_NOSTORE; the last CTA finishes the detector row (detect_finish).
+template <typename Real, int LOG_L1, int C, int E, bool DET = false>
 __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(PassArgs a) {
     using B = Block<Real, LOG_L1, C, E>;
     using Cx = typename B::Cx;
-    constexpr int L = B::L;
     // Four-step factor W_M^(n2 k1) of column n2 = col0 + c at the frequency
     // k1 = freq_base(tp) | freq_off(r) held by register r: the thread's part
     // W^(n2 freq_base(tp)) times the register's part W^(n2 freq_off(r)) (E
@@ -590,8 +674,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 
     unsigned char *tab0 = smraw + (B::SMEM + 15) / 16 * 16;
 
+    int64_t t_first = blockIdx.x, t_end = tiles, t_step = gridDim.x;
+    if constexpr (DET) {
+        const int64_t per = (tiles + gridDim.x - 1) / gridDim.x;
+        t_first = int64_t(blockIdx.x) * per;
+        t_end = t_first + per < tiles ? t_first + per : tiles;
+        t_step = 1;
+    }
     int parity = 0;
-    for (int64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, parity ^= 1) {
+    for (int64_t tile = t_first; tile < t_end; tile += t_step, parity ^= 1) {
         // factor tables, double-buffered by tile parity
         double2 *tx = reinterpret_cast<double2 *>(tab0 + parity * PAR);
         double2 *ty = tx + C * XP;
@@ -639,14 +730,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
                 }
             }
             B::inverse(sm, tp, v, tw);
-        } else {
+        } else if constexpr (!DET) {
 #pragma unroll
             for (int r = 0; r < E; ++r)
                 v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[int64_t(B::first_pos(tp, r)) << log_n2];
         }
-        if (flags & PF_TRANS)
+        // the detection variant runs the inverse only: no transmission, no forward
+        if (!DET && (flags & PF_TRANS))
             apply_trans_e<E>(a.tr, [&](int r) { return base + (int64_t(B::first_pos(tp, r)) << log_n2) + col; }, v);
-        if (flags & PF_FWD) {
+        if (!DET && (flags & PF_FWD)) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
                 const Lf *vc = vec + c * EP;
@@ -665,11 +757,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[int64_t(B::last_pos(tp, r)) << log_n2] = v[r];
         } else {
+            if constexpr (DET) detect_bin<B>(a.det, base, col, tp, v, log_n2);
+            if (!DET || !(flags & PF_NOSTORE)) {
 #pragma unroll
-            for (int r = 0; r < E; ++r) gout[int64_t(B::first_pos(tp, r)) << log_n2] = v[r];
+                for (int r = 0; r < E; ++r) gout[int64_t(B::first_pos(tp, r)) << log_n2] = v[r];
+            }
         }
         if (!paired) __syncthreads();
     }
+    if constexpr (DET) detect_finish(a.det);
 }
 
 // exp(2 pi i G N1^2 k2s^2) for every register (r, tp) of the row kernel
@@ -697,12 +793,37 @@ template <typename K> static cudaError_t prep(K kernel, size_t smem) {
 }
 
 // persistent grid: as many CTAs as fit on the device at once, capped by the work
-template <typename K> static int64_t resident_ctas(K kernel, int threads, size_t smem) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
+template <typename K> static int64_t resident_ctas(K kernel, int threads, size_t smem, int dev) {
+    int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     return int64_t(sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
+}
+
+// Launch set-up of one kernel, per device: the dynamic shared-memory limit is
+// a per-device attribute of the kernel and the resident CTA count depends on
+// the device, so both are taken once for each device the kernel launches on
+// (the device current at the launch). cap[1] is the CTA count at the
+// second shared-memory size (the column kernel without its factor tables).
+constexpr int LAUNCH_MAX_DEVICES = 64;
+struct LaunchSetup {
+    cudaError_t attr = cudaSuccess;
+    int64_t cap[2] = {1, 1};
+};
+template <typename K>
+static const LaunchSetup *launch_setup(K kernel, int threads, size_t smem, size_t smem2, LaunchSetup *table,
+                                       std::once_flag *once) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= LAUNCH_MAX_DEVICES) return nullptr;
+    std::call_once(once[dev], [&] {
+        LaunchSetup &st = table[dev];
+        st.attr = prep(kernel, smem > smem2 ? smem : smem2);
+        if (st.attr == cudaSuccess) {
+            st.cap[0] = resident_ctas(kernel, threads, smem, dev);
+            st.cap[1] = resident_ctas(kernel, threads, smem2, dev);
+        }
+    });
+    return &table[dev];
 }
 
 template <int L> constexpr int n_vec() { return 64 + ((L >> 6) > 0 ? (L >> 6) : 1); }
@@ -712,9 +833,12 @@ template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t ro
     using B = Block<Real, LG, 1, E>;
     auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
     const size_t smem = (B::SMEM + 15) / 16 * 16 + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * 16;
-    static cudaError_t attr = prep(k, smem);
-    if (attr != cudaSuccess) return attr;
-    static int64_t cap = resident_ctas(k, B::NT, smem);
+    static LaunchSetup setup[LAUNCH_MAX_DEVICES];
+    static std::once_flag once[LAUNCH_MAX_DEVICES];
+    const LaunchSetup *st = launch_setup(k, B::NT, smem, smem, setup, once);
+    if (!st) return cudaErrorInvalidDevice;
+    if (st->attr != cudaSuccess) return st->attr;
+    const int64_t cap = st->cap[0];
     const int64_t rows = a.n >> LG;
     k<<<dim3(unsigned(rows < cap ? rows : cap)), dim3(B::NT), smem, s>>>(a);
     count_launch();
@@ -737,21 +861,28 @@ constexpr int col_c(int log_l) {
 // segments, measured 26 % and 13 % faster than 32-byte ones at 2^28 and 2^24)
 constexpr int col_c64(int log_l) { return log_l == 10 ? 16 : log_l == 11 ? 8 : col_c(log_l); }
 
-template <typename Real, int LG, int C, int E> static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
+template <typename Real, int LG, int C, int E, bool DET = false>
+static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
-    auto k = col_pass_kernel<Real, LG, C, E>;
+    auto k = col_pass_kernel<Real, LG, C, E, DET>;
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
     const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, 16>();
-    static cudaError_t attr = prep(k, tab);
-    if (attr != cudaSuccess) return attr;
-    static int64_t cap_tab = resident_ctas(k, B::NT, tab);
-    static int64_t cap_plain = resident_ctas(k, B::NT, plain);
+    static LaunchSetup setup[LAUNCH_MAX_DEVICES];
+    static std::once_flag once[LAUNCH_MAX_DEVICES];
+    const LaunchSetup *st = launch_setup(k, B::NT, tab, plain, setup, once);
+    if (!st) return cudaErrorInvalidDevice;
+    if (st->attr != cudaSuccess) return st->attr;
     const bool tables = a.flags & (PF_TW | PF_TWI);
-    const int64_t cap = tables ? cap_tab : cap_plain;
+    const int64_t cap = tables ? st->cap[0] : st->cap[1];
     const int64_t tiles = (a.n >> LG) / C;
     if ((int64_t(1) << a.log_n2) < C) return cudaErrorInvalidValue;  // fewer columns per batch than a tile
-    k<<<dim3(unsigned(tiles < cap ? tiles : cap)), dim3(B::NT), tables ? tab : plain, s>>>(a);
+    int64_t grid = tiles < cap ? tiles : cap;
+    if constexpr (DET) {  // contiguous tile ranges: no CTA without tiles
+        const int64_t per = (tiles + grid - 1) / grid;
+        grid = (tiles + per - 1) / per;
+    }
+    k<<<dim3(unsigned(grid)), dim3(B::NT), tables ? tab : plain, s>>>(a);
     count_launch();
     return cudaGetLastError();
 }

@@ -73,6 +73,23 @@ RSW_HD inline void stage_tw_entry(int log_l, int s, int max_ls, int rb, int64_t 
     }
 }
 
+// How a complex64 lifting entry (rsw_block_fft.cuh) covers angles beyond a
+// quarter turn. Twiddle q of a radix-R stage, W_{RS}^{jq} with j < S, has an
+// angle in (-2 pi q / R, 0]:
+//   mode 0 (4q <= R):  within (-pi/2, 0]: the entry is the rotation itself;
+//   mode 1 (2q <= R):  within (-pi, 0]: the entry rotates by the angle + pi/2
+//                      and the kernel follows it with a fixed quarter turn -i;
+//   mode 2 (q > R/2):  the entry carries a half-turn flag in the low bit of a.
+// The low factors W^{(j mod 64) q} of factored stages (S >= 256) stay below
+// a quarter turn: mode 0.
+RSW_HD constexpr int tw_mode(int q, int r) { return 4 * q <= r ? 0 : 2 * q <= r ? 1 : 2; }
+RSW_HD inline int stage_tw_mode(int log_l, int s, int max_ls, int rb, int64_t k) {
+    const int64_t R = int64_t(1) << stage_lr(log_l, s, rb), S = int64_t(1) << stage_ls(log_l, s, rb);
+    if (stage_direct(log_l, s, max_ls, rb)) return tw_mode(int(k / S + 1), int(R));
+    if (k < (R - 1) * 64) return 0;
+    return tw_mode(int((k - (R - 1) * 64) / (S / 64) + 1), int(R));
+}
+
 // Frequency index held at block position p after the forward stages. The map
 // is a permutation of the bits of p, so positions with disjoint bits map to
 // frequencies with disjoint bits: digitrev(a | b) == digitrev(a) | digitrev(b).

@@ -1,6 +1,7 @@
 """Multi-rank logic on CPU (gloo, world size 2): source sharding covers every
-source exactly once with balanced cost, and the detector all-reduce of the
-per-rank weighted sums equals the single-process sum."""
+source exactly once with balanced cost, and the all-reduce of the per-rank
+spectrum-weighted FP64 detector arrays ([phase][pix], one per source, from
+the CPU oracle on fields of two lengths) equals the single-process sum."""
 
 import os
 import socket
@@ -32,40 +33,66 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def fake_detector(energy, n_phase=3, n_pix=5):
-    # stands in for one source's detector output: smooth in energy and pixel
-    p = np.arange(n_phase)[:, None]
-    j = np.arange(n_pix)[None, :]
-    return np.cos(energy * 1e-4 + p) * (1 + j) / energy
+def _sources():
+    """Energies on fields of two lengths (the batched-config shape, scaled
+    down): per source its case, energy, spectrum weight and cost N * steps."""
+    from rave_sim_b200 import workloads
+
+    out = []
+    for case, energies, weights in workloads.batched_energies(
+            count=6, log_min=10, log_max=11, window=float(1 << 11) * 20e-9, nr_steps=2, phase_steps=3):
+        for e, w in zip(energies, weights):
+            out.append((case, float(e), float(w)))
+    return out
 
 
-def _worker(rank, world, port, energies, weights, q):
+def _detector(case, energy):
+    """One source's FP64 detector array [phase][pix] from the CPU oracle."""
+    from oracle import bigwave_np as bw
+    from rave_sim_b200 import workloads
+
+    return bw.run_simulation(dict(case, energy=energy, db=workloads.db_table(energy)))
+
+
+def _worker(rank, world, port, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        mine = shard_sources([1.0] * len(energies), world)[rank]
-        acc = torch.zeros((3, 5), dtype=torch.float64)
+        src = _sources()
+        costs = [float(c["sim_params"]["N"]) for c, _, _ in src]
+        mine = shard_sources(costs, world)[rank]
+        acc = None
         for i in mine:
-            acc += weights[i] * torch.from_numpy(fake_detector(energies[i]))
+            case, e, w = src[i]
+            d = torch.from_numpy(w * _detector(case, e))
+            acc = d if acc is None else acc + d
+        if acc is None:
+            acc = torch.zeros_like(torch.from_numpy(_detector(*src[0][:2])))
         reduce_detector(acc)
-        q.put((rank, acc.numpy()))
+        q.put((rank, sorted(mine), acc.numpy()))
     finally:
         dist.destroy_process_group()
 
 
 def test_detector_allreduce_gloo_world2():
-    energies = np.linspace(20000.0, 70000.0, 11)
-    weights = np.linspace(1.0, 2.0, 11)
-    ref = sum(w * fake_detector(e) for e, w in zip(energies, weights))
+    src = _sources()
+    assert len({int(c["sim_params"]["N"]) for c, _, _ in src}) == 2
+    ref = sum(w * _detector(c, e) for c, e, w in src)
+    assert ref.ndim == 2 and ref.shape[0] == 3 and ref.max() > 0
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, energies, weights, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    res = dict(q.get(timeout=120) for _ in procs)
+    res = {}
+    for _ in procs:
+        r, mine, acc = q.get(timeout=300)
+        res[r] = (mine, acc)
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
+    assert sorted(res[0][0] + res[1][0]) == list(range(len(src)))  # every source once
+    assert res[0][0] and res[1][0]
     for r in range(2):
-        np.testing.assert_allclose(res[r], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+        np.testing.assert_allclose(res[r][1], ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())

@@ -98,3 +98,44 @@ def test_noalloc_call_leaves_free_memory_unchanged():
     torch.cuda.synchronize()
     free_after, _ = torch.cuda.mem_get_info()
     assert free_after == free_before
+
+
+def test_noalloc_lengths_keep_their_own_tables():
+    # each length and dtype has its own tables: alternating lengths, then
+    # coming back to the first one, gives the plan's spectrum every time
+    lib = L.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    for i, (n, code) in enumerate([(1 << 10, L.RSW_C64), (1 << 12, L.RSW_C64), (1 << 10, L.RSW_C64),
+                                   (1 << 15, L.RSW_C128), (1 << 12, L.RSW_C64), (1 << 10, L.RSW_C64)]):
+        x = _field(n, 100 + i, code)
+        ref = _plan_fft(lib, x, code)
+        out = torch.empty_like(x)
+        assert lib.rsw_fft_forward_noalloc(x.data_ptr(), out.data_ptr(), n, code, stream) == L.RSW_OK
+        torch.cuda.synchronize()
+        assert _rel(out, ref) < TOL[code], f"call {i}: n={n}"
+
+
+def test_noalloc_first_call_for_a_length_refused_while_capturing():
+    # the first call for a length and dtype builds its tables, which a graph
+    # capture would only record: refused with RSW_ERR_INVALID, nothing launched
+    lib = L.load()
+    n, code = 1 << 5, L.RSW_C128  # a length no other test uses
+    x = _field(n, 3, code)
+    out = torch.empty_like(x)
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        st = lib.rsw_fft_forward_noalloc(x.data_ptr(), out.data_ptr(), n, code, s.cuda_stream)
+        torch.mul(x, 1.0, out=out)  # keep the graph non-empty
+        g.capture_end()
+    assert st == L.RSW_ERR_INVALID
+    assert b"capturing" in lib.rsw_last_error()
+    del g
+    # outside the capture the same call builds the tables and succeeds
+    ref = _plan_fft(lib, x, code)
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.rsw_fft_forward_noalloc(x.data_ptr(), out.data_ptr(), n, code, stream) == L.RSW_OK
+    torch.cuda.synchronize()
+    assert _rel(out, ref) < TOL[code]
