@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    ap.add_argument("--no-gpu-baseline", action="store_true",
+                    help="skip the reference's cuFFT fast-wave path on the same workload")
     a = ap.parse_args()
     if a.dtype is None:
         a.dtype = "c16" if a.workload == "talbot_lau" else "c8"
@@ -214,6 +216,37 @@ def reference_arm(args, rank, ws):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def gpu_baseline(args, value, det):
+    """The reference's GPU path (fast-wave's kernels and cuFFT, compiled
+    unmodified, on fast-wave's schedule) timed on the same workload and
+    energies in its own process (baseline/fastwave). Never falls back to the
+    engine's kernels: without the prebuilt library the block says why."""
+    lib = ROOT / "baseline" / "_ref" / "libfastwave_harness.so"
+    if args.workload not in ("talbot_lau", "thick_sample"):
+        return {"unavailable": f"no fast-wave baseline for the {args.workload} workload"}
+    if args.logn > 30:
+        return {"unavailable": "fast-wave indexes fields with int (N > 2^30 is out of its range)"}
+    if not lib.exists():
+        return {"unavailable": "baseline/_ref/libfastwave_harness.so is not built (needs the reference checkout)"}
+    with tempfile.TemporaryDirectory() as td:
+        out = Path(td) / "det.npy"
+        cmd = [sys.executable, "-m", "baseline.fastwave.run", "--workload", args.workload, "--dtype", args.dtype,
+               "--logn", str(args.logn), "--energies", str(args.energies), "--repeats", "1", "--warmup", "1",
+               "--detector", str(out)]
+        r = subprocess.run(cmd, cwd=str(ROOT), capture_output=True, text=True)
+        if r.returncode != 0 or not r.stdout.strip():
+            tail = (r.stderr or r.stdout).strip().splitlines()[-1:] or ["no output"]
+            return {"unavailable": f"fast-wave run failed (exit {r.returncode}): {tail[0][:200]}"}
+        b = json.loads(r.stdout.strip().splitlines()[-1])
+        fw = np.load(out)
+    b["ratio"] = value / b["value"]
+    if det is not None and fw.shape == det.shape and np.linalg.norm(det) > 0:
+        # fast-wave follows its own discrete rules (grating coordinates, cutoff,
+        # binning): information, not a parity figure
+        b["detector_rel_l2_vs_engine"] = float(np.linalg.norm(fw - det) / np.linalg.norm(det))
+    return b
 
 
 # ------------------------------------------------------------------ jobs
@@ -447,6 +480,10 @@ def main():
                "sample": f"{k} grating split steps (mask + FFT + transfer + iFFT) at N=2^{lg} "
                          f"{args.dtype}, FP64 numpy/scipy oracle, 1 thread, {dt:.1f} s"}
 
+    gpu_base = None
+    if rank == 0 and ws == 1 and not args.no_gpu_baseline:
+        gpu_base = gpu_baseline(args, value, acc.cpu().numpy() if len(groups) == 1 else None)
+
     if rank == 0:
         cfg = {"workload": workload_name(args),
                "fields": [{"n": g["n"], "energies": len(g["energies"]), "split_steps": k}
@@ -474,6 +511,7 @@ def main():
             "clocks": clk,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "gpu_baseline": gpu_base,
         }
         if precision is not None:
             line["precision"] = precision

@@ -192,6 +192,85 @@ def lookup_deltabeta(db_table, material) -> complex:
     return cands[0][1]
 
 
+def deltabeta_vector(material_slots, db_table) -> np.ndarray:
+    """The per-run deltabeta vector (rsw_source_run.deltabeta): the materials
+    of every element in descriptor order, looked up in a subconfig deltabeta
+    table."""
+    vals = []
+    for slots in material_slots:
+        vals.extend(lookup_deltabeta(db_table, m) for m in slots)
+    return np.ascontiguousarray(np.asarray(vals, dtype=np.complex128).reshape(-1))
+
+
+def sim_descriptor(config: dict, grids: Optional[dict], code: int, angles: Sequence[float]):
+    """The C descriptors (rsw_sim_desc and its rsw_element array) of a
+    setup in the reference's config.yaml schema. Returns (desc, elements,
+    keep, material_slots): ``keep`` holds the arrays the descriptors point to
+    (keep it alive while they are used), ``material_slots`` the materials of
+    each element in the order of the per-run deltabeta vector."""
+    grids = grids or {}
+    sp = config["sim_params"]
+    n = int(sp["N"])
+    dx = float(sp["dx"])
+    els = config["elements"]
+    if len(angles) != len(els) + 1:
+        raise ValueError("cutoff_angles must have len(elements) + 1 entries")
+    keep = []
+    arr = (L.Element * max(len(els), 1))()
+    material_slots = []  # per element: list of materials in deltabeta order
+    for i, el in enumerate(els):
+        e = arr[i]
+        xp = np.ascontiguousarray(np.asarray(el["x_positions"], dtype=np.float64).reshape(-1))
+        keep.append(xp)
+        e.n_x_positions = len(xp)
+        e.x_positions = xp.ctypes.data_as(L._DP)
+        e.z_start = float(el["z_start"])
+        t = el["type"]
+        if t in ("grating", "dba_grating"):
+            e.type = L.RSW_EL_GRATING if t == "grating" else L.RSW_EL_DBA_GRATING
+            e.thickness = float(el["thickness"])
+            e.substrate_thickness = float(el["substrate_thickness"])
+            e.nr_steps = int(el["nr_steps"])
+            if t == "grating":
+                e.pitch = float(el["pitch"])
+                e.dc[0], e.dc[1] = (float(v) for v in el["dc"])
+            else:
+                e.pitch = float(el["pitch0"])
+                e.pitch1 = float(el["pitch1"])
+                e.dc[0], e.dc[1] = (float(v) for v in el["dc0"])
+                e.dc1[0], e.dc1[1] = (float(v) for v in el["dc1"])
+            material_slots.append([el.get("mat_a"), el.get("mat_b"), el.get("mat_substrate")])
+        elif t == "sample":
+            g = np.ascontiguousarray(np.asarray(grids[i]))
+            if g.dtype != np.int8 or g.ndim != 2:
+                raise ValueError("sample grids must be 2-D int8 arrays")
+            keep.append(g)
+            e.type = L.RSW_EL_SAMPLE
+            e.pixel_size_x = float(el["pixel_size_x"])
+            e.pixel_size_z = float(el["pixel_size_z"])
+            e.grid_z, e.grid_x = g.shape
+            e.grid = g.ctypes.data_as(C.POINTER(C.c_int8))
+            e.n_materials = len(el["materials"])
+            material_slots.append(list(el["materials"]))
+        else:
+            raise ValueError(f"unknown element type {t!r}")
+    ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float64))
+    keep.append(ang)
+    d = L.SimDesc()
+    d.n = n
+    d.dtype = code
+    d.dx = dx
+    d.z_detector = float(sp["z_detector"])
+    d.detector_size = float(sp["detector_size"])
+    d.pixel_size_x = float(sp["detector_pixel_size_x"])
+    d.pixel_size_y = float(sp["detector_pixel_size_y"])
+    d.chunk_size = int(sp.get("chunk_size", n))
+    d.n_elements = len(els)
+    d.elements = arr
+    d.cutoff_angles = ang.ctypes.data_as(L._DP)
+    return d, arr, keep, material_slots
+
+
 class Simulation:
     """A rave-sim setup on the fused engine.
 
@@ -203,69 +282,13 @@ class Simulation:
     def __init__(self, config: dict, grids: Optional[dict] = None, dtype=None,
                  cutoff_angles: Optional[Sequence[float]] = None):
         self._lib = L.load()
-        grids = grids or {}
         sp = config["sim_params"]
         self.config = config
         self.code = dtype_code(dtype if dtype is not None else config.get("dtype", "c16"))
         self.n = int(sp["N"])
         self.dx = float(sp["dx"])
         angles = list(cutoff_angles if cutoff_angles is not None else config["cutoff_angles"])
-        els = config["elements"]
-        if len(angles) != len(els) + 1:
-            raise ValueError("cutoff_angles must have len(elements) + 1 entries")
-        self._keep = []
-        arr = (L.Element * max(len(els), 1))()
-        self.material_slots = []  # per element: list of materials in deltabeta order
-        for i, el in enumerate(els):
-            e = arr[i]
-            xp = np.ascontiguousarray(np.asarray(el["x_positions"], dtype=np.float64).reshape(-1))
-            self._keep.append(xp)
-            e.n_x_positions = len(xp)
-            e.x_positions = xp.ctypes.data_as(L._DP)
-            e.z_start = float(el["z_start"])
-            t = el["type"]
-            if t in ("grating", "dba_grating"):
-                e.type = L.RSW_EL_GRATING if t == "grating" else L.RSW_EL_DBA_GRATING
-                e.thickness = float(el["thickness"])
-                e.substrate_thickness = float(el["substrate_thickness"])
-                e.nr_steps = int(el["nr_steps"])
-                if t == "grating":
-                    e.pitch = float(el["pitch"])
-                    e.dc[0], e.dc[1] = (float(v) for v in el["dc"])
-                else:
-                    e.pitch = float(el["pitch0"])
-                    e.pitch1 = float(el["pitch1"])
-                    e.dc[0], e.dc[1] = (float(v) for v in el["dc0"])
-                    e.dc1[0], e.dc1[1] = (float(v) for v in el["dc1"])
-                self.material_slots.append([el.get("mat_a"), el.get("mat_b"), el.get("mat_substrate")])
-            elif t == "sample":
-                g = np.ascontiguousarray(np.asarray(grids[i]))
-                if g.dtype != np.int8 or g.ndim != 2:
-                    raise ValueError("sample grids must be 2-D int8 arrays")
-                self._keep.append(g)
-                e.type = L.RSW_EL_SAMPLE
-                e.pixel_size_x = float(el["pixel_size_x"])
-                e.pixel_size_z = float(el["pixel_size_z"])
-                e.grid_z, e.grid_x = g.shape
-                e.grid = g.ctypes.data_as(C.POINTER(C.c_int8))
-                e.n_materials = len(el["materials"])
-                self.material_slots.append(list(el["materials"]))
-            else:
-                raise ValueError(f"unknown element type {t!r}")
-        ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float64))
-        self._keep.append(ang)
-        d = L.SimDesc()
-        d.n = self.n
-        d.dtype = self.code
-        d.dx = self.dx
-        d.z_detector = float(sp["z_detector"])
-        d.detector_size = float(sp["detector_size"])
-        d.pixel_size_x = float(sp["detector_pixel_size_x"])
-        d.pixel_size_y = float(sp["detector_pixel_size_y"])
-        d.chunk_size = int(sp.get("chunk_size", self.n))
-        d.n_elements = len(els)
-        d.elements = arr
-        d.cutoff_angles = ang.ctypes.data_as(L._DP)
+        d, arr, self._keep, self.material_slots = sim_descriptor(config, grids, self.code, angles)
         self._elements = arr
         h = C.c_void_p()
         L.check(self._lib.rsw_sim_create(C.byref(h), C.byref(d)))
@@ -289,10 +312,7 @@ class Simulation:
         return s.value
 
     def deltabeta_vector(self, db_table) -> np.ndarray:
-        vals = []
-        for slots in self.material_slots:
-            vals.extend(lookup_deltabeta(db_table, m) for m in slots)
-        return np.ascontiguousarray(np.asarray(vals, dtype=np.complex128).reshape(-1))
+        return deltabeta_vector(self.material_slots, db_table)
 
     def reset(self):
         L.check(self._lib.rsw_sim_reset(self._h, _stream_ptr()))
