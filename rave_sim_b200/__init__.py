@@ -10,3 +10,4 @@ from .retrieval import dark_field, signal_retrieval_least_squares  # noqa: F401
 
 __all__ = ["Plan", "Simulation", "run_case", "wavelength_from_energy", "RswError", "load_library",
            "signal_retrieval_least_squares", "dark_field"]
+from .geometry import compute_cutoff_angles, grid_density_check, max_dx  # noqa: E402,F401

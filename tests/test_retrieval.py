@@ -1,12 +1,37 @@
 """Phase-stepping signal retrieval (the crack-simulation notebook's
-signal_retrieval_least_squares, notebooks/Crack_simulation.ipynb cell 4) on
-the device against the numpy restatement in oracle/retrieval_np.py."""
+signal_retrieval_least_squares, notebooks/Crack_simulation.ipynb cell 4): the
+numpy restatement in oracle/retrieval_np.py and the device implementation,
+both against the notebook function itself (tests/golden/retrieval.npz, made
+by tests/golden/make_retrieval_golden.py, which runs the notebook cell)."""
 
 import numpy as np
 import pytest
 
-from conftest import load_case
+from conftest import GOLDEN, load_case
 from oracle import retrieval_np as ro
+
+
+def golden_cases():
+    """(data [steps][pixels], period, dabs, dphase, dvis, mean chi2) of the
+    notebook function's runs."""
+    d = np.load(GOLDEN / "retrieval.npz")
+    return [(d[f"data_{i}"], float(d[f"period_{i}"]), d[f"dabs_{i}"], d[f"dphase_{i}"], d[f"dvis_{i}"],
+             float(d[f"chi2_{i}"])) for i in range(int(d["n_cases"]))]
+
+
+def check_against_golden(got, ref, chi2=True):
+    data, period, dabs, dphase, dvis, c2 = ref
+    np.testing.assert_allclose(got[0], dabs, rtol=1e-12)
+    np.testing.assert_allclose(got[1], dphase, atol=1e-12)
+    np.testing.assert_allclose(got[2], dvis, rtol=1e-11)
+    if chi2:
+        assert got[3] == pytest.approx(c2, rel=1e-9, abs=1e-24)
+
+
+def test_oracle_matches_notebook_function():
+    for ref in golden_cases():
+        got = ro.signal_retrieval_least_squares(ref[0], period=ref[1], axis=0)
+        check_against_golden(got, ref)
 
 
 def curves(n_pix, nsteps, period, seed):
@@ -95,3 +120,13 @@ def test_device_rejects_bad_step_counts():
         signal_retrieval_least_squares(np.ones((10, 2)), axis=-1)
     with pytest.raises(RswError):
         signal_retrieval_least_squares(np.ones((10, 65)), axis=-1)
+
+
+@gpu
+def test_device_matches_notebook_function():
+    _need_cuda()
+    from rave_sim_b200 import signal_retrieval_least_squares
+
+    for ref in golden_cases():
+        got = signal_retrieval_least_squares(ref[0], period=ref[1], axis=0)
+        check_against_golden(got, ref, chi2=ref[0].shape[0] > 3)
