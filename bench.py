@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--compare-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the built-in schedule instead of timing the candidates first")
     ap.add_argument("--no-gpu-baseline", action="store_true",
                     help="skip the reference's cuFFT fast-wave path on the same workload")
     a = ap.parse_args()
@@ -96,15 +98,21 @@ def measured_peak_hbm():
 
 
 def ncu_traffic(kernel: str, dtype: str, logn: int):
-    """dram bytes per launch from the committed ncu summary (scaled to 2^logn)."""
+    """(dram bytes per launch, how) from the committed ncu summary: the
+    capture at this size when there is one, else the 2^24 capture scaled by
+    the samples per launch."""
     if not PROFILE_TRAFFIC.exists():
-        return None
+        return None, None
+    lines = {}
     for line in PROFILE_TRAFFIC.read_text().splitlines():
         f = line.split()
         if len(f) >= 4 and not line.startswith("#") and f[0] == kernel and f[1] == dtype:
-            cap_logn, by = int(f[2]), float(f[3])
-            return by * 2.0 ** (logn - cap_logn)
-    return None
+            lines[int(f[2])] = float(f[3])
+    if logn in lines:
+        return lines[logn], f"ncu capture at 2^{logn}"
+    if 24 in lines:
+        return lines[24] * 2.0 ** (logn - 24), f"ncu capture at 2^24 scaled by 2^{logn - 24}"
+    return None, None
 
 
 class ClockSampler:
@@ -319,6 +327,16 @@ def main():
     lib = rsw.load_library()
     s_bytes = 16 if args.dtype == "c16" else 8
     groups = build_groups(args, ws, rank, args.dtype)
+    tuning = {}
+    if not args.no_autotune:
+        # the schedule of each field length chosen by timing (registered for
+        # the simulations created below)
+        from rave_sim_b200 import autotune
+
+        for n_g in sorted({int(g["case"]["sim_params"]["N"]) for g in groups}):
+            r = autotune.tune(n_g, args.dtype, reps=5, save=False)
+            tuning[str(n_g)] = {"choice": r["best"], "ms_per_split_step": r["ms_per_split_step"],
+                                "candidates": len(r["tried"])}
     for g in groups:
         g["sim"] = rsw.Simulation(g["case"], grids=g["grids"], dtype=args.dtype)
         g["n"] = int(g["case"]["sim_params"]["N"])
@@ -450,7 +468,8 @@ def main():
                 "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": algo_bytes,
-                "traffic": ncu_traffic(dom, args.dtype, int(round(math.log2(n)))), "kernels": kinds}
+                "kernels": kinds}
+    roofline["traffic"], roofline["traffic_source"] = ncu_traffic(dom, args.dtype, int(round(math.log2(n))))
 
     # ---- mixed precision against the complex128 run of the same step
     precision = None
@@ -492,7 +511,8 @@ def main():
                "split_steps_per_bench_step": int(sum(steps_g)) * ws,
                "l2_policy": "inputs larger than L2" if n * s_bytes > (126 << 20) else
                             "field smaller than L2 (no flush)",
-               "parallelism": f"dp{ws} (energies sharded, detector all-reduce)"}
+               "parallelism": f"dp{ws} (energies sharded, detector all-reduce)",
+               "schedule": {"autotuned": tuning} if tuning else "built-in"}
         if args.workload == "talbot_lau":
             cfg.update({"n": n, "energies_per_rank": len(gd["energies"]), "field_bytes": n * s_bytes,
                         "l2_policy": "inputs larger than L2 (field 2^24 c128 = 256 MiB)"

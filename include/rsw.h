@@ -53,7 +53,7 @@ int rsw_abi_version(void);
 /* Number of kernels this library launched since load (all threads). */
 uint64_t rsw_launch_count(void);
 /* sizeof of the ABI structs, for bindings to verify their layouts:
- * 0 rsw_element, 1 rsw_sim_desc, 2 rsw_source, 3 rsw_source_run. */
+ * 0 rsw_element, 1 rsw_sim_desc, 2 rsw_source, 3 rsw_source_run, 4 rsw_tuning. */
 size_t rsw_struct_size(int which);
 
 /* Photon wavelength in metres for an energy in eV, evaluated exactly as the
@@ -73,6 +73,38 @@ rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype);
 rsw_status rsw_plan_destroy(rsw_plan plan);
 rsw_status rsw_plan_info(rsw_plan plan, int64_t *n, int *dtype, int *log_rows,
                          int *log_cols, int64_t *scratch_bytes);
+
+/* ------------------------------------------------------------ tuning
+ * The choices cuFFT makes inside cufftPlan1d (fast-wave/src/fft.cpp:8) are
+ * explicit here: the level split and the samples per thread of each kernel.
+ * levels: 0 = the default choice, 1 = one row pass, 2 = columns of 2^log_rows
+ * samples and rows of the rest, 3 = columns of 2^log_rows, a middle level of
+ * 2^log_mid and rows of the rest. row_e, col_e, mid_e: samples per thread of
+ * the row, column and middle kernels (8, 16 or 32 where a kernel exists;
+ * 0 = default). An unavailable choice returns RSW_ERR_INVALID. */
+typedef struct {
+    int levels;
+    int log_rows;
+    int log_mid;
+    int row_e, col_e, mid_e;
+} rsw_tuning;
+rsw_status rsw_plan_create_tuned(rsw_plan *out, int64_t n, int dtype, const rsw_tuning *tuning);
+/* The plan's effective choices. */
+rsw_status rsw_plan_tuning(rsw_plan plan, rsw_tuning *tuning);
+/* Register the tuning that later rsw_plan_create / rsw_sim_create calls use
+ * for this n and dtype (process-wide; tuning == NULL removes it). The
+ * RSW_SPLIT, RSW_SPLIT3, RSW_ROW_E and RSW_COL_E environment variables take
+ * precedence over registered tunings. */
+rsw_status rsw_set_tuning(int64_t n, int dtype, const rsw_tuning *tuning);
+/* No counterpart in the reference (cuFFT tunes inside its plan call): time
+ * every available tuning of (n, dtype) on one steady-state split step of a
+ * simulation (reps timed steps each, after two untimed ones, on `stream`,
+ * over a field of n samples allocated here) and return the fastest in *best
+ * and its milliseconds per split step in *best_ms. tried / tried_ms (may be
+ * NULL) receive up to max_tried candidates and their times, *n_tried the
+ * number timed. Synchronises `stream`. */
+rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double *best_ms,
+                        rsw_tuning *tried, double *tried_ms, int max_tried, int *n_tried, void *stream);
 
 /* fast-wave FFT<S>::forward / inverse (src/fft.cpp:28-44); natural order in and
  * out; in == out allowed. */
@@ -114,6 +146,17 @@ rsw_status rsw_fft_forward_noalloc(const void *d_in, void *d_out, int64_t n, int
  * be h_in. N is a power of two >= 256. Synchronises `stream` before returning. */
 rsw_status rsw_fft_host(const void *h_in, void *h_out, void *h_scratch, int64_t n, int dtype, int inverse,
                         int64_t device_bytes, void *stream);
+
+/* Transfer function of rsw_propagate and of simulations. RSW_PROP_FRESNEL is
+ * the reference's (big-wave/propagation.py:124-128, fast-wave
+ * fwcuda/kernels.cu:52) and the default. RSW_PROP_EXACT has no counterpart in
+ * the reference: the exact angular-spectrum kernel exp(-i 2 pi dz
+ * sqrt(1/wl^2 - f^2)), the constant -2 pi dz / wl taken out as for the
+ * Fresnel kernel and the rest, 2 pi dz f^2 / (1/wl + sqrt(1/wl^2 - f^2)),
+ * evaluated per sample in FP64; evanescent components (f^2 >= 1/wl^2) are
+ * set to zero. Slower than the Fresnel kernel (no chirp factorisation). */
+typedef enum { RSW_PROP_FRESNEL = 0, RSW_PROP_EXACT = 1 } rsw_propagator;
+rsw_status rsw_plan_set_propagator(rsw_plan plan, int mode);
 
 /* big-wave propagation.propagate (big-wave/propagation.py:100-138) and
  * fast-wave propagate<S> (fast-wave/src/simulation.cpp:34-40): u <- iFFT(H * FFT(u))
@@ -289,6 +332,9 @@ rsw_status rsw_sim_timing(rsw_sim sim, int kind, double *ms, int64_t *launches);
  * (np.stack(entries, axis=-1)) and their z to host memory; NULL outputs are
  * skipped; it synchronises. */
 rsw_status rsw_sim_set_history(rsw_sim sim, double history_dz);
+/* The transfer function of the following runs (rsw_propagator; default
+ * RSW_PROP_FRESNEL, the reference's). */
+rsw_status rsw_sim_set_propagator(rsw_sim sim, int mode);
 rsw_status rsw_sim_history(rsw_sim sim, double *h_history, double *h_z, int64_t *n_entries,
                            void *stream);
 

@@ -55,6 +55,7 @@ class Sim:
     psy: float
     wl: float
     chunk_size: int
+    propagator: str = "fresnel"  # or "exact": the opt-in angular-spectrum kernel
 
 
 # --------------------------------------------------------------------------
@@ -96,13 +97,35 @@ def transfer_function_exact(n: int, dx: float, wl: float, dz: float) -> np.ndarr
     return np.exp(-1j * 2 * np.pi / wl * dz) * np.exp(1j * th)
 
 
+def transfer_function_angular(n: int, dx: float, wl: float, dz: float) -> np.ndarray:
+    """The exact angular-spectrum kernel of the engine's opt-in propagator
+    (no counterpart in the reference, whose kernel is the Fresnel one):
+    exp(-i 2 pi dz sqrt(1/wl^2 - fx^2)) as the same constant
+    exp(-i 2 pi dz / wl) times exp(i phi), phi = 2 pi dz fx^2 /
+    (1/wl + sqrt(1/wl^2 - fx^2)) (no cancellation), fx as in
+    ``transfer_function``; evanescent components (fx^2 >= 1/wl^2) are zero.
+    The FP64 operations are those of the engine, in the same order."""
+    fx = (signed_fft_index(n) * (1.0 / n)) / dx
+    f2 = fx * fx
+    inv_wl = 1.0 / wl
+    d = inv_wl * inv_wl - f2
+    prop = d > 0
+    phi = np.where(prop, ((2.0 * np.pi) * dz) * f2 / (inv_wl + np.sqrt(np.where(prop, d, 1.0))), 0.0)
+    return np.where(prop, np.exp(-1j * 2 * np.pi / wl * dz) * np.exp(1j * phi), 0.0)
+
+
 def propagate(u, U, sim: Sim, dz: float, cutoff_freq: float, skip_fft=False, exact_phase=False):
     """``propagate`` (big-wave/propagation.py:100-138). Returns (u_new, U_new)
-    with ``U_new`` the spectrum of ``u_new`` as in the reference."""
+    with ``U_new`` the spectrum of ``u_new`` as in the reference. With
+    ``sim.propagator == "exact"`` the transfer function is the engine's
+    opt-in angular-spectrum kernel instead of the reference's."""
     if not skip_fft:
         U = spfft.fft(u)
     # ``chunk *= H``: computed in complex128, stored in the field's dtype
-    tf = transfer_function_exact if exact_phase else transfer_function
+    if sim.propagator == "exact":
+        tf = transfer_function_angular
+    else:
+        tf = transfer_function_exact if exact_phase else transfer_function
     U = (U * tf(len(u), sim.dx, sim.wl, dz)).astype(U.dtype, copy=False)
     rng = cutoff_zero_range(len(u), cutoff_freq, sim.dx)
     if rng is not None:
@@ -285,7 +308,8 @@ def make_sim(case) -> Sim:
                psx=float(sp["detector_pixel_size_x"]),
                psy=float(sp["detector_pixel_size_y"]),
                wl=wavelength_from_energy(float(case["energy"])),
-               chunk_size=int(sp["chunk_size"]))
+               chunk_size=int(sp["chunk_size"]),
+               propagator=str(case.get("propagator", "fresnel")))
 
 
 def history_zs(dz, hdz):

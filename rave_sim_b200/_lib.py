@@ -17,6 +17,7 @@ RSW_OK, RSW_ERR_INVALID, RSW_ERR_UNSUPPORTED, RSW_ERR_CUDA, RSW_ERR_NOMEM, RSW_E
 RSW_C128, RSW_C64 = 0, 1
 RSW_EL_GRATING, RSW_EL_DBA_GRATING, RSW_EL_SAMPLE = 0, 1, 2
 RSW_SRC_PLANE, RSW_SRC_POINT, RSW_SRC_VECTOR = 0, 1, 2
+RSW_PROP_FRESNEL, RSW_PROP_EXACT = 0, 1
 
 STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "NOMEM", 5: "TIMEOUT"}
 
@@ -87,6 +88,17 @@ class SourceRun(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("levels", C.c_int),
+        ("log_rows", C.c_int),
+        ("log_mid", C.c_int),
+        ("row_e", C.c_int),
+        ("col_e", C.c_int),
+        ("mid_e", C.c_int),
+    ]
+
+
 _P = C.c_void_p
 _D = C.c_double
 _I64 = C.c_int64
@@ -100,6 +112,11 @@ SIGNATURES = {
     "rsw_struct_size": (C.c_size_t, [C.c_int]),
     "rsw_energy_to_wavelength": (C.c_double, [C.c_double]),
     "rsw_plan_create": (C.c_int, [C.POINTER(_P), _I64, C.c_int]),
+    "rsw_plan_create_tuned": (C.c_int, [C.POINTER(_P), _I64, C.c_int, C.POINTER(Tuning)]),
+    "rsw_plan_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "rsw_set_tuning": (C.c_int, [_I64, C.c_int, C.POINTER(Tuning)]),
+    "rsw_autotune": (C.c_int, [_I64, C.c_int, C.c_int, C.POINTER(Tuning), _DP, C.POINTER(Tuning), _DP,
+                               C.c_int, C.POINTER(C.c_int), _P]),
     "rsw_plan_destroy": (C.c_int, [_P]),
     "rsw_plan_info": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.POINTER(_I64)]),
@@ -117,6 +134,8 @@ SIGNATURES = {
     "rsw_detector_geometry": (C.c_int, [_I64, _D, _D, _D, _D, C.POINTER(_I64), C.POINTER(_I64), _DP, _DP]),
     "rsw_signal_retrieval": (C.c_int, [_P, _I64, C.c_int, _D, _P, _P, _P, _P, _P]),
     "rsw_sim_set_history": (C.c_int, [_P, _D]),
+    "rsw_sim_set_propagator": (C.c_int, [_P, C.c_int]),
+    "rsw_plan_set_propagator": (C.c_int, [_P, C.c_int]),
     "rsw_sim_history": (C.c_int, [_P, _DP, _DP, C.POINTER(_I64), _P]),
     "rsw_sim_create": (C.c_int, [C.POINTER(_P), C.POINTER(SimDesc)]),
     "rsw_sim_destroy": (C.c_int, [_P]),
@@ -149,7 +168,7 @@ def load(path: os.PathLike | None = None) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    for i, st in enumerate((Element, SimDesc, Source, SourceRun)):
+    for i, st in enumerate((Element, SimDesc, Source, SourceRun, Tuning)):
         if lib.rsw_struct_size(i) != C.sizeof(st):
             raise ImportError(f"ABI mismatch for {st.__name__}: C {lib.rsw_struct_size(i)} "
                               f"vs ctypes {C.sizeof(st)}")

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -127,9 +128,17 @@ static cplx material_factor(double delta, double beta, double t, double wl) {
 }
 
 // Propagator scalars of propagate() (big-wave/propagation.py:74-137).
-static PropArgs make_prop(int64_t n, double dx, double wl, double dz, double cutoff_freq, bool apply_h) {
+// exact: the angular-spectrum kernel instead of the Fresnel one (opt-in, no
+// counterpart in the reference): phi = 2 pi dz fx^2 / (1/wl + sqrt(1/wl^2 - fx^2))
+// beyond the same constant -2 pi dz / wl.
+static PropArgs make_prop(int64_t n, double dx, double wl, double dz, double cutoff_freq, bool apply_h,
+                          bool exact = false) {
     PropArgs p{};
     p.has_h = apply_h ? 1 : 0;
+    p.exact = exact ? 1 : 0;
+    p.inv_wl = 1.0 / wl;
+    p.inv_wl2 = p.inv_wl * p.inv_wl;
+    p.z2pi = (2.0 * M_PI) * dz;
     p.c = (M_PI * wl) * dz;
     const double phi = ((-2.0 * M_PI) / wl) * dz;
     p.A = make_double2(std::cos(phi), std::sin(phi));
@@ -302,6 +311,7 @@ struct rsw_plan_s {
     int log_nb = 0, log_nr = 0;  // N2 = Nb * Nr: middle level (0: two-level) and row-kernel length
     int device = 0;
     int row_e = 16, col_e = 16, mid_e = 16;  // elements per thread of the row / column / middle kernels
+    int prop_mode = RSW_PROP_FRESNEL;        // transfer function of propagate and of simulations
     DevBuf tw_row, tw_col, tw_mid, tw4_lo, tw4_hi, tw4b_lo, tw4b_hi;
     int tw4_shift = 0, tw4b_shift = 0;
     DevBuf scratch;                                       // N samples, for the natural-order APIs
@@ -420,7 +430,30 @@ template <typename T> static rsw_status plan_tables(rsw_plan_s *p) {
 // that three levels, N = N1 x Nb x Nr, with rows of the row kernel's maximum
 // length and the rest split evenly between the outer column level and the
 // middle level (both run by the column kernel).
-static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb, int *lr) {
+// A split from a tuning (levels 1..3): single level; columns of 2^log_rows
+// and rows of the rest; columns, a middle level of 2^log_mid and rows.
+static rsw_status tuned_split(int lg, int dtype, const rsw_tuning &t, int *l1, int *lb, int *lr) {
+    const int row_max = dtype == RSW_C128 ? ROW_MAX_C128 : ROW_MAX_C64;
+    const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
+    *lb = 0;
+    if (t.levels == 1) {
+        if (lg > row_max) return fail(RSW_ERR_INVALID, "tuning: 2^%d is above the single-level limit 2^%d", lg, row_max);
+        *l1 = 0;
+        *lr = lg;
+        return RSW_OK;
+    }
+    const int a = t.log_rows, b = t.levels == 3 ? t.log_mid : 0, c = lg - a - b;
+    if (a < 4 || a > col_max || (t.levels == 3 && (b < 4 || b > col_max)) || c < 7 || c > row_max ||
+        (t.levels != 2 && t.levels != 3))
+        return fail(RSW_ERR_INVALID, "tuning: split %d levels, %d / %d / %d of 2^%d is not available", t.levels, a, b,
+                    c, lg);
+    *l1 = a;
+    *lb = b;
+    *lr = c;
+    return RSW_OK;
+}
+
+static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb, int *lr, const rsw_tuning *t) {
     if (n < 16 || (n & (n - 1)) != 0)
         return fail(RSW_ERR_UNSUPPORTED, "N = %lld: this version supports powers of two >= 16", (long long)n);
     int lg = 0;
@@ -429,6 +462,7 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
     const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
     *log_n = lg;
     *lb = 0;
+    if (t && t->levels != 0) return tuned_split(lg, dtype, *t, l1, lb, lr);
     // RSW_SPLIT3 = "l1,lb,lr" forces a three-level split (tests and tuning sweeps)
     const char *ov3 = std::getenv("RSW_SPLIT3");
     if (ov3 && *ov3) {
@@ -509,19 +543,74 @@ static int env_int(const char *name, int dflt) {
     const char *v = std::getenv(name);
     return v && *v ? std::atoi(v) : dflt;
 }
-static void choose_tuning(rsw_plan_s *p) {
+// Samples per thread the kernels are built for: multi-level rows 16 from
+// 2^7, 32 from 2^9, 8 for 2^11..2^13 (single-level rows 16); columns (and
+// middle levels) 16, 8 for 2^8..2^11, 32 from 2^9.
+static bool row_e_ok(int log_nr, bool multi, int e) {
+    if (!multi) return e == 16;
+    return (e == 16 && log_nr >= 7) || (e == 32 && log_nr >= 9) || (e == 8 && log_nr >= 11 && log_nr <= 13);
+}
+static bool col_e_ok(int log_l, int e) {
+    return (e == 16 && log_l >= 4) || (e == 8 && log_l >= 8 && log_l <= 11) || (e == 32 && log_l >= 9);
+}
+
+static rsw_status choose_tuning(rsw_plan_s *p, const rsw_tuning *t) {
     auto pick = [](int log_l, int dflt) { return log_l >= 9 ? dflt : 16; };
     p->row_e = pick(p->log_nr, 16);
     const bool c128 = p->dtype == RSW_C128;
     const int l1 = p->log_n1;
     p->col_e = (c128 && l1 >= 8 && l1 <= 11) || (!c128 && (l1 == 9 || (l1 == 10 && p->log_nb == 0))) ? 8 : pick(l1, 16);
     p->mid_e = pick(p->log_nb, 16);
+    if (t) {
+        const bool multi = p->log_n1 > 0;
+        if (t->row_e && !row_e_ok(p->log_nr, multi, t->row_e))
+            return fail(RSW_ERR_INVALID, "tuning: rows of 2^%d have no kernel with %d samples per thread", p->log_nr,
+                        t->row_e);
+        if (t->col_e && (!multi || !col_e_ok(p->log_n1, t->col_e)))
+            return fail(RSW_ERR_INVALID, "tuning: no column kernel of 2^%d with %d samples per thread", p->log_n1,
+                        t->col_e);
+        if (t->mid_e && (!p->three() || !col_e_ok(p->log_nb, t->mid_e)))
+            return fail(RSW_ERR_INVALID, "tuning: no middle kernel of 2^%d with %d samples per thread", p->log_nb,
+                        t->mid_e);
+        if (t->row_e) p->row_e = t->row_e;
+        if (t->col_e) p->col_e = t->col_e;
+        if (t->mid_e) p->mid_e = t->mid_e;
+        return RSW_OK;
+    }
     const int re = env_int("RSW_ROW_E", 0), ce = env_int("RSW_COL_E", 0);
     if ((re == 16 || re == 32) && p->log_nr >= 9) p->row_e = re;
     if (ce == 16 || (ce == 32 && p->log_n1 >= 9)) p->col_e = ce;
     // 8 samples per thread: multi-level rows of 2^11..2^13, columns of 2^8..2^11
     if (re == 8 && p->log_n1 > 0 && p->log_nr >= 11 && p->log_nr <= 13) p->row_e = 8;
     if (ce == 8 && p->log_n1 >= 8 && p->log_n1 <= 11) p->col_e = 8;
+    return RSW_OK;
+}
+
+// Tunings registered for later plans (rsw_set_tuning), per length and dtype.
+struct TuningEntry {
+    int64_t n;
+    int dtype;
+    rsw_tuning t;
+};
+static std::mutex g_tuning_mutex;
+static std::vector<TuningEntry> g_tunings;
+static bool registered_tuning(int64_t n, int dtype, rsw_tuning *t) {
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    for (const TuningEntry &e : g_tunings)
+        if (e.n == n && e.dtype == dtype) {
+            *t = e.t;
+            return true;
+        }
+    return false;
+}
+// the tuning environment variables of tests and sweeps take precedence over
+// registered tunings
+static bool env_overrides() {
+    for (const char *v : {"RSW_SPLIT", "RSW_SPLIT3", "RSW_ROW_E", "RSW_COL_E"}) {
+        const char *x = std::getenv(v);
+        if (x && *x) return true;
+    }
+    return false;
 }
 
 // Arguments of the outer column pass (and of single-level row passes).
@@ -668,7 +757,7 @@ static rsw_status run_mid(const rsw_plan_s *p, const PassArgs &base, bool forwar
 // samples) and switch `pr` to the chirp form. Multi-level plans only: the
 // spectrum index of a row sample is kbase + M k2 with M = N1 Nb.
 static rsw_status prepare_chirp(const rsw_plan_s *p, PropArgs &pr, void *table, cudaStream_t s) {
-    if (p->log_n1 == 0 || !pr.has_h) return RSW_OK;
+    if (p->log_n1 == 0 || !pr.has_h || pr.exact) return RSW_OK;
     double g_hi, g_lo;
     chirp_constant(pr, p->n, &g_hi, &g_lo);
     const double msq = std::ldexp(1.0, 2 * (p->log_n1 + p->log_nb));  // exact power of two
@@ -678,6 +767,41 @@ static rsw_status prepare_chirp(const rsw_plan_s *p, PropArgs &pr, void *table, 
     pr.g_hi = g_hi;
     pr.g_lo = g_lo;
     pr.h3 = table;
+    return RSW_OK;
+}
+
+// The launches of one split step from `a.in` (NULL with ones: the plane
+// wave) into `a.out`, with a.tr / a.pr set: multi-level plans run the column
+// pass (the inverse of the previous step when the input is in the "mid"
+// representation, transmission, forward), the middle passes of three-level
+// plans around the row pass, and leave the "mid" representation; single-level
+// plans run one row pass and leave the field in natural order.
+static rsw_status launch_split_step(const rsw_plan_s *P, PassArgs a, bool mid_in, bool ones, cudaStream_t st,
+                                    TimingLog *tl, bool *mid_out) {
+    const bool trans = a.tr.kind != TR_NONE;
+    if (P->log_n1 > 0) {
+        const void *out = a.out;
+        a.flags = (mid_in ? col_inv(P) : 0) | PF_FWD | PF_TW | (trans ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
+        const PropArgs keep = a.pr;
+        a.pr = PropArgs{};
+        CHECK(run_col(P, a, st, tl));
+        a.in = out;
+        a.tr.kind = TR_NONE;
+        if (P->three()) CHECK(run_mid(P, a, true, st, tl));
+        a.pr = keep;
+        PassArgs r = row_level(P, a);
+        r.flags = PF_FWD | PF_INV | row_tw(P, true, true);
+        CHECK(run_row(P, r, st, tl));
+        if (P->three()) {
+            a.pr = PropArgs{};
+            CHECK(run_mid(P, a, false, st, tl));
+        }
+        *mid_out = true;
+    } else {
+        a.flags = PF_FWD | PF_INV | PF_SCALE | (trans ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
+        CHECK(run_row(P, a, st, tl));
+        *mid_out = false;
+    }
     return RSW_OK;
 }
 
@@ -694,16 +818,17 @@ size_t rsw_struct_size(int which) {
     case 1: return sizeof(rsw_sim_desc);
     case 2: return sizeof(rsw_source);
     case 3: return sizeof(rsw_source_run);
+    case 4: return sizeof(rsw_tuning);
     default: return 0;
     }
 }
 
-rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
+static rsw_status create_plan(rsw_plan *out, int64_t n, int dtype, const rsw_tuning *t) {
     if (!out) return fail(RSW_ERR_INVALID, "out is NULL");
     *out = nullptr;
     if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
     int lg, l1, lb, lr;
-    CHECK(plan_split(n, dtype, &lg, &l1, &lb, &lr));
+    CHECK(plan_split(n, dtype, &lg, &l1, &lb, &lr, t));
     std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
     if (!p) return fail(RSW_ERR_NOMEM, "host allocation failed");
     p->n = n;
@@ -714,9 +839,149 @@ rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
     p->log_nr = lr;
     p->log_n2 = lb + lr;
     CU(cudaGetDevice(&p->device));
-    choose_tuning(p.get());
+    CHECK(choose_tuning(p.get(), t));
     CHECK(p->dbl() ? plan_tables<double>(p.get()) : plan_tables<float>(p.get()));
     *out = p.release();
+    return RSW_OK;
+}
+
+rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
+    rsw_tuning reg{};
+    const bool use = !env_overrides() && registered_tuning(n, dtype, &reg);
+    return create_plan(out, n, dtype, use ? &reg : nullptr);
+}
+
+rsw_status rsw_plan_create_tuned(rsw_plan *out, int64_t n, int dtype, const rsw_tuning *t) {
+    return create_plan(out, n, dtype, t);
+}
+
+rsw_status rsw_plan_tuning(rsw_plan p, rsw_tuning *t) {
+    if (!p || !t) return fail(RSW_ERR_INVALID, "NULL argument");
+    t->levels = p->log_n1 == 0 ? 1 : p->three() ? 3 : 2;
+    t->log_rows = p->log_n1;
+    t->log_mid = p->log_nb;
+    t->row_e = p->row_e;
+    t->col_e = p->log_n1 > 0 ? p->col_e : 0;
+    t->mid_e = p->three() ? p->mid_e : 0;
+    return RSW_OK;
+}
+
+rsw_status rsw_set_tuning(int64_t n, int dtype, const rsw_tuning *t) {
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    g_tunings.erase(std::remove_if(g_tunings.begin(), g_tunings.end(),
+                                   [&](const TuningEntry &e) { return e.n == n && e.dtype == dtype; }),
+                    g_tunings.end());
+    if (t) g_tunings.push_back(TuningEntry{n, dtype, *t});
+    return RSW_OK;
+}
+
+// The plan choice cuFFT makes inside cufftPlan1d (fast-wave/src/fft.cpp:8),
+// made here by measurement: every split and samples-per-thread combination
+// the kernels are built for is timed on one steady-state split step of a
+// simulation (inverse column pass, grating transmission, forward column
+// pass, [middle passes,] row pass with the chirp transfer function) over a
+// field of n samples on the device, and the fastest is returned.
+rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double *best_ms, rsw_tuning *tried,
+                        double *tried_ms, int max_tried, int *n_tried, void *stream) {
+    if (!best) return fail(RSW_ERR_INVALID, "best is NULL");
+    if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
+    if (n < 16 || (n & (n - 1)) != 0)
+        return fail(RSW_ERR_UNSUPPORTED, "N = %lld: this version supports powers of two >= 16", (long long)n);
+    if (reps < 1) reps = 1;
+    int lg = 0;
+    while ((int64_t(1) << lg) < n) ++lg;
+    const int row_max = dtype == RSW_C128 ? ROW_MAX_C128 : ROW_MAX_C64;
+    const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
+    std::vector<rsw_tuning> cands;
+    if (lg <= row_max) cands.push_back(rsw_tuning{1, 0, 0, 16, 0, 0});
+    if (lg <= row_max + col_max) {
+        for (int l1 = 4; l1 <= col_max; ++l1) {
+            const int lr = lg - l1;
+            if (lr < 7 || lr > row_max) continue;
+            for (int re : {16, 32, 8})
+                for (int ce : {16, 8, 32})
+                    if (row_e_ok(lr, true, re) && col_e_ok(l1, ce)) cands.push_back(rsw_tuning{2, l1, 0, re, ce, 0});
+        }
+    } else {
+        // three levels: rows of the longest row kernel (fewest samples in
+        // the two column levels), the column lengths and kernels varied
+        for (int l1 = 4; l1 <= col_max; ++l1) {
+            const int lb = lg - row_max - l1;
+            if (lb < 4 || lb > col_max) continue;
+            for (int ce : {16, 8})
+                for (int me : {16, 8})
+                    if (col_e_ok(l1, ce) && col_e_ok(lb, me)) cands.push_back(rsw_tuning{3, l1, lb, 16, ce, me});
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t elem = dtype == RSW_C128 ? 16 : 8;
+    DevBuf field;
+    CHECK(field.alloc(size_t(n) * elem));
+    {
+        cudaError_t e = launch_fill_ones(field.p, n, dtype == RSW_C128, s);
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "fill: %s", cudaGetErrorString(e));
+    }
+    // a grating sub-step at 46 keV on a 2 nm grid, 10 um thick, no cutoff
+    const double dx = 2e-9, wl = 2.6953e-11, dz = 1e-5;
+    TransArgs tr{};
+    tr.kind = TR_GRATING;
+    tr.fa = make_double2(0.9, 0.1);
+    tr.fb = make_double2(1.0, 0.0);
+    tr.pitch0 = 4.2e-6;
+    tr.inv_pitch0 = 1.0 / tr.pitch0;
+    tr.dc0 = 0.5;
+    tr.half_dc0 = 0.25;
+    tr.xstart0 = -double(n / 2) * dx;
+    tr.step0 = dx;
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    struct Events {
+        cudaEvent_t a, b;
+        ~Events() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev{e0, e1};
+    double best_t = 1e300;
+    int count = 0;
+    for (const rsw_tuning &c : cands) {
+        rsw_plan raw = nullptr;
+        if (create_plan(&raw, n, dtype, &c) != RSW_OK) continue;
+        std::unique_ptr<rsw_plan_s> pl(raw);
+        DevBuf h3;
+        if (pl->log_n1 > 0 && h3.alloc(size_t(int64_t(1) << pl->log_nr) * 16) != RSW_OK) continue;
+        PassArgs a = base_args(pl.get());
+        a.in = field.p;
+        a.out = field.p;
+        a.tr = tr;
+        a.pr = make_prop(n, dx, wl, dz, 1e300, true);
+        if (prepare_chirp(pl.get(), a.pr, h3.p, s) != RSW_OK) continue;
+        bool mid = false, ok = true;
+        for (int w = 0; w < 2 && ok; ++w) ok = launch_split_step(pl.get(), a, pl->log_n1 > 0, false, s, nullptr, &mid) == RSW_OK;
+        if (!ok) continue;
+        CU(cudaEventRecord(e0, s));
+        for (int r = 0; r < reps && ok; ++r)
+            ok = launch_split_step(pl.get(), a, pl->log_n1 > 0, false, s, nullptr, &mid) == RSW_OK;
+        CU(cudaEventRecord(e1, s));
+        CU(cudaEventSynchronize(e1));
+        if (!ok) continue;
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        const double per = double(ms) / reps;
+        if (tried && tried_ms && count < max_tried) {
+            tried[count] = c;
+            tried_ms[count] = per;
+        }
+        ++count;
+        if (per < best_t) {
+            best_t = per;
+            CHECK(rsw_plan_tuning(pl.get(), best));
+        }
+    }
+    if (n_tried) *n_tried = count;
+    if (count == 0) return fail(RSW_ERR_CUDA, "autotune: no candidate ran for N = 2^%d", lg);
+    if (best_ms) *best_ms = best_t;
     return RSW_OK;
 }
 
@@ -732,6 +997,16 @@ rsw_status rsw_plan_info(rsw_plan p, int64_t *n, int *dtype, int *log_rows, int 
     if (log_rows) *log_rows = p->log_n1;
     if (log_cols) *log_cols = p->log_n2;
     if (scratch) *scratch = int64_t(p->scratch.bytes);
+    return RSW_OK;
+}
+
+rsw_status rsw_plan_set_propagator(rsw_plan p, int mode) {
+    if (!p) return fail(RSW_ERR_INVALID, "plan is NULL");
+    if (mode != RSW_PROP_FRESNEL && mode != RSW_PROP_EXACT) return fail(RSW_ERR_INVALID, "unknown propagator %d", mode);
+    // the exact kernel runs the per-sample row kernels (16 samples per thread)
+    if (mode == RSW_PROP_EXACT && p->log_n1 > 0 && p->row_e != 16)
+        return fail(RSW_ERR_UNSUPPORTED, "the exact propagator needs rows of 16 samples per thread");
+    p->prop_mode = mode;
     return RSW_OK;
 }
 
@@ -935,9 +1210,9 @@ rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, dou
     if (!(dx > 0) || !(wl > 0)) return fail(RSW_ERR_INVALID, "dx and wl must be positive");
     cudaStream_t s = (cudaStream_t)stream;
     PassArgs a = base_args(p);
-    a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0);
+    a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0, p->prop_mode == RSW_PROP_EXACT);
     const bool two = p->log_n1 > 0;
-    if (two && a.pr.has_h) {
+    if (two && a.pr.has_h && !a.pr.exact) {
         CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_nr) * 16));  // 16-byte entries
         CHECK(prepare_chirp(p, a.pr, p->h3_call.p, s));
     }
@@ -1287,7 +1562,7 @@ struct Runner {
 
     // chirp table for a distance dz at this run's wavelength (built on first use)
     rsw_status chirp_for(PropArgs &pr, double dz) {
-        if (P->log_n1 == 0 || !pr.has_h) return RSW_OK;
+        if (P->log_n1 == 0 || !pr.has_h || pr.exact) return RSW_OK;
         size_t slot = 0;
         while (slot < chirp_dz.size() && chirp_dz[slot] != dz) ++slot;
         const bool fresh = slot == chirp_dz.size();
@@ -1323,36 +1598,12 @@ struct Runner {
     rsw_status step_to(const TransArgs &tr, double dz, double cutoff, int dst, bool commit) {
         PassArgs a = base_args(P);
         a.tr = tr;
-        a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0);
+        a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0, P->prop_mode == RSW_PROP_EXACT);
         CHECK(chirp_for(a.pr, dz));
+        a.in = ones ? nullptr : bp(cur);
+        a.out = bp(dst);
         bool now_mid;
-        if (P->log_n1 > 0) {
-            a.in = ones ? nullptr : bp(cur);
-            a.out = bp(dst);
-            a.flags = (mid ? col_inv(P) : 0) | PF_FWD | PF_TW | (tr.kind != TR_NONE ? PF_TRANS : 0) |
-                      (ones ? PF_ONES : 0);
-            PropArgs keep = a.pr;
-            a.pr = PropArgs{};
-            CHECK(run_col(P, a, st, &S->tl));
-            a.in = bp(dst);
-            a.tr.kind = TR_NONE;
-            if (P->three()) CHECK(run_mid(P, a, true, st, &S->tl));
-            a.pr = keep;
-            PassArgs r = row_level(P, a);
-            r.flags = PF_FWD | PF_INV | row_tw(P, true, true);
-            CHECK(run_row(P, r, st, &S->tl));
-            if (P->three()) {
-                a.pr = PropArgs{};
-                CHECK(run_mid(P, a, false, st, &S->tl));
-            }
-            now_mid = true;
-        } else {
-            a.in = ones ? nullptr : bp(cur);
-            a.out = bp(dst);
-            a.flags = PF_FWD | PF_INV | PF_SCALE | (tr.kind != TR_NONE ? PF_TRANS : 0) | (ones ? PF_ONES : 0);
-            CHECK(run_row(P, a, st, &S->tl));
-            now_mid = false;
-        }
+        CHECK(launch_split_step(P, a, mid, ones, st, &S->tl, &now_mid));
         if (commit) {
             cur = dst;
             ones = false;
@@ -1754,6 +2005,11 @@ rsw_status rsw_sim_timing(rsw_sim S, int kind, double *ms, int64_t *launches) {
     if (ms) *ms = S->tl.ms[kind];
     if (launches) *launches = S->tl.launches[kind];
     return RSW_OK;
+}
+
+rsw_status rsw_sim_set_propagator(rsw_sim S, int mode) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    return rsw_plan_set_propagator(S->plan, mode);
 }
 
 rsw_status rsw_sim_set_history(rsw_sim S, double history_dz) {

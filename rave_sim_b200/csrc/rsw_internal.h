@@ -55,6 +55,11 @@ struct PropArgs {
     int chirp;
     double g_hi, g_lo;
     const void *h3;
+    // Exact angular-spectrum kernel (opt-in; not in the reference): H = A
+    // exp(i phi), phi = z2pi fx^2 / (inv_wl + sqrt(inv_wl2 - fx^2)), evaluated
+    // per sample (no chirp form); evanescent fx^2 >= inv_wl2 is zeroed.
+    int exact;
+    double inv_wl, inv_wl2, z2pi;
 };
 
 enum PassFlags : int {

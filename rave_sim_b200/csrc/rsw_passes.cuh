@@ -255,11 +255,31 @@ __device__ __forceinline__ double2 cis_turns(double t) {
     sincospi(2.0 * t, &s, &c);
     return make_double2(c, s);
 }
+// Phase of the exact angular-spectrum kernel beyond the constant -2 pi dz / wl
+// (carried in A): 2 pi dz (1/wl - sqrt(1/wl^2 - fx^2)) written without the
+// cancellation as 2 pi dz fx^2 / (1/wl + sqrt(1/wl^2 - fx^2)), fx as in
+// prop_phase. False for an evanescent component (fx^2 >= 1/wl^2).
+__device__ __forceinline__ bool exact_phase(const PropArgs &p, int64_t ks, double *phi) {
+    const double fx = __dmul_rn(div_rn(double(ks), p.dx, p.rdx), p.fac);
+    const double f2 = __dmul_rn(fx, fx);
+    const double d = __dsub_rn(p.inv_wl2, f2);
+    if (!(d > 0.0)) return false;
+    *phi = __ddiv_rn(__dmul_rn(p.z2pi, f2), __dadd_rn(p.inv_wl, __dsqrt_rn(d)));
+    return true;
+}
+// the per-sample phase of the transfer function: Fresnel (the reference's) or
+// exact; false: the component is zeroed
+__device__ __forceinline__ bool prop_phase_any(const PropArgs &p, int64_t ks, double *phi) {
+    if (p.exact) return exact_phase(p, ks, phi);
+    *phi = prop_phase(p, ks);
+    return true;
+}
 __device__ __forceinline__ double2 prop_apply(const PropArgs &p, int64_t k, int64_t ks, double2 U) {
     if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) return make_double2(0.0, 0.0);
     if (!p.has_h) return U;
-    double s, c;
-    sincos_phase(prop_phase(p, ks), &s, &c);
+    double s, c, ph;
+    if (!prop_phase_any(p, ks, &ph)) return make_double2(0.0, 0.0);
+    sincos_phase(ph, &s, &c);
     const double2 H = make_double2(p.A.x * c - p.A.y * s, p.A.x * s + p.A.y * c);
     return cmul(U, H);
 }
@@ -268,8 +288,9 @@ __device__ __forceinline__ double2 prop_apply(const PropArgs &p, int64_t k, int6
 __device__ __forceinline__ float2 prop_apply(const PropArgs &p, int64_t k, int64_t ks, float2 U) {
     if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) return make_float2(0.f, 0.f);
     if (!p.has_h) return U;
-    double s, c;
-    sincos_phase(prop_phase(p, ks), &s, &c);
+    double s, c, ph;
+    if (!prop_phase_any(p, ks, &ph)) return make_float2(0.f, 0.f);
+    sincos_phase(ph, &s, &c);
     return rot(U, lift_of(make_double2(p.A.x * c - p.A.y * s, p.A.x * s + p.A.y * c)));
 }
 
@@ -844,10 +865,14 @@ template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t ro
     count_launch();
     return cudaGetLastError();
 }
+// PF_TWF (rows of three-level plans) takes the TWF variant, for the chirp
+// form and for the per-sample transfer function (exact kernel) alike; rows of
+// multi-level plans hold at least 2^7 samples
 template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
-    if constexpr (CH) {
-        if (a.flags & PF_TWF) return row_launch<Real, LG, E, true, true>(a, s);
+    if constexpr (LG >= 7) {
+        if (a.flags & PF_TWF) return row_launch<Real, LG, E, CH, true>(a, s);
     }
+    if (a.flags & PF_TWF) return cudaErrorInvalidValue;
     return row_launch<Real, LG, E, CH, false>(a, s);
 }
 

@@ -18,7 +18,9 @@ namespace rsw {
     case L: return chirp ? cudaErrorInvalidValue : row_impl<R, L, 16, false>(a, s);
 
 cudaError_t launch_row_pass_f32(const PassArgs &a, int e, cudaStream_t s) {
-    const bool chirp = a.log_n1 > 0;
+    // multi-level rows take the chirp form of the Fresnel kernel; the exact
+    // kernel and single-level rows evaluate the transfer function per sample
+    const bool chirp = a.log_n1 > 0 && !a.pr.exact;
     switch (a.log_n2) {
         RSW_ROW_CASE_S(float, 4) RSW_ROW_CASE_S(float, 5) RSW_ROW_CASE_S(float, 6) RSW_ROW_CASE16(float, 7)
         RSW_ROW_CASE16(float, 8) RSW_ROW_CASE(float, 9) RSW_ROW_CASE(float, 10) RSW_ROW_CASE8(float, 11)

@@ -18,7 +18,9 @@ namespace rsw {
     case L: return chirp ? cudaErrorInvalidValue : row_impl<R, L, 16, false>(a, s);
 
 cudaError_t launch_row_pass_f64(const PassArgs &a, int e, cudaStream_t s) {
-    const bool chirp = a.log_n1 > 0;
+    // multi-level rows take the chirp form of the Fresnel kernel; the exact
+    // kernel and single-level rows evaluate the transfer function per sample
+    const bool chirp = a.log_n1 > 0 && !a.pr.exact;
     switch (a.log_n2) {
             RSW_ROW_CASE_S(double, 4) RSW_ROW_CASE_S(double, 5) RSW_ROW_CASE_S(double, 6)
             RSW_ROW_CASE16(double, 7) RSW_ROW_CASE16(double, 8) RSW_ROW_CASE(double, 9)

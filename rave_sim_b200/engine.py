@@ -73,6 +73,20 @@ def _dptr(t) -> int:
     return int(t.data_ptr())
 
 
+PROPAGATORS = {"fresnel": L.RSW_PROP_FRESNEL, "exact": L.RSW_PROP_EXACT}
+
+
+def propagator_code(name) -> int:
+    """'fresnel' (the reference's transfer function, the default) or 'exact'
+    (the angular-spectrum kernel, opt-in)."""
+    if name is None:
+        return L.RSW_PROP_FRESNEL
+    try:
+        return PROPAGATORS[str(name).lower()]
+    except KeyError:
+        raise ValueError(f"unknown propagator {name!r}: use 'fresnel' or 'exact'") from None
+
+
 def _pair(c: complex):
     arr = (C.c_double * 2)(float(np.real(c)), float(np.imag(c)))
     return arr
@@ -81,12 +95,19 @@ def _pair(c: complex):
 class Plan:
     """FFT plan of length ``n`` (a power of two) for c16 or c8 fields."""
 
-    def __init__(self, n: int, dtype="c16"):
+    def __init__(self, n: int, dtype="c16", tuning: Optional[dict] = None):
+        """``tuning``: explicit schedule choices (rave_sim_b200.autotune.FIELDS;
+        default: the registered or built-in choice)."""
         self._lib = L.load()
         self.n = int(n)
         self.code = dtype_code(dtype)
         h = C.c_void_p()
-        L.check(self._lib.rsw_plan_create(C.byref(h), self.n, self.code))
+        if tuning is None:
+            L.check(self._lib.rsw_plan_create(C.byref(h), self.n, self.code))
+        else:
+            t = L.Tuning(*(int(tuning.get(f, 0)) for f in ("levels", "log_rows", "log_mid", "row_e", "col_e",
+                                                             "mid_e")))
+            L.check(self._lib.rsw_plan_create_tuned(C.byref(h), self.n, self.code, C.byref(t)))
         self._h = h
 
     def close(self):
@@ -122,6 +143,11 @@ class Plan:
         out = x if out is None else out
         L.check(self._lib.rsw_fft_inverse(self._h, self._check_field(x), self._check_field(out), _stream_ptr()))
         return out
+
+    def set_propagator(self, name: str):
+        """Transfer function of ``propagate``: 'fresnel' (the reference's,
+        default) or 'exact' (angular spectrum)."""
+        L.check(self._lib.rsw_plan_set_propagator(self._h, propagator_code(name)))
 
     def propagate(self, u, U=None, *, dx, wl, dz, cutoff_freq, skip_fft=False):
         """big-wave ``propagate`` (propagation.py:100-138); ``u`` updated in
@@ -280,7 +306,7 @@ class Simulation:
     """
 
     def __init__(self, config: dict, grids: Optional[dict] = None, dtype=None,
-                 cutoff_angles: Optional[Sequence[float]] = None):
+                 cutoff_angles: Optional[Sequence[float]] = None, propagator: Optional[str] = None):
         self._lib = L.load()
         sp = config["sim_params"]
         self.config = config
@@ -297,6 +323,9 @@ class Simulation:
         L.check(self._lib.rsw_sim_shape(self._h, C.byref(nps), C.byref(npix), C.byref(_)))
         self.nr_phase_steps = nps.value
         self.n_pix = npix.value
+        prop = propagator if propagator is not None else config.get("propagator")
+        if prop is not None:
+            L.check(self._lib.rsw_sim_set_propagator(self._h, propagator_code(prop)))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -89,3 +89,17 @@ def test_oracle_history_matches_reference(name):
     assert h.shape == d["history"].shape
     assert rel_l2(h, d["history"]) < 1e-13
     assert rel_l2(det, d["detected"]) < 1e-13
+
+
+def test_angular_kernel_reduces_to_fresnel_at_small_frequencies():
+    # sqrt(1/wl^2 - f^2) = 1/wl - wl f^2 / 2 - wl^3 f^4 / 8 - ...: the exact
+    # kernel's phase exceeds the Fresnel one by 2 pi dz wl^3 f^4 / 8 to leading order
+    n, dx, wl, dz = 1 << 12, 2e-9, 2.6953e-11, 0.0818
+    ha = bw.transfer_function_angular(n, dx, wl, dz)
+    hf = bw.transfer_function(n, dx, wl, dz)
+    fx = np.fft.fftfreq(n, dx)
+    d = np.angle(ha * np.conj(hf))
+    small = np.abs(fx) < 0.05 / dx
+    pred = 2 * np.pi * dz * wl ** 3 * fx ** 4 / 8
+    np.testing.assert_allclose(d[small], pred[small], rtol=1e-3, atol=1e-9)
+    assert np.all(np.abs(np.abs(ha) - 1) < 1e-14)
