@@ -62,11 +62,15 @@ double rsw_energy_to_wavelength(double energy_ev);
 
 /* ------------------------------------------------------------ FFT plans
  * Replaces fast-wave's FFT<S> (fast-wave/src/fft.hpp:9-24, src/fft.cpp:6-48):
- * a 1-D complex FFT of length N (a power of two, 16 <= N <= 2^38 for C64 and
- * 2^35 for C128), forward unnormalised, inverse scaled by 1/N (the
- * reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length. Up to
- * 2^26 (C64) / 2^24 (C128) a split step costs two passes over the field,
- * beyond that four (three-level plans). log_rows + log_cols = log2 N.
+ * a 1-D complex FFT of length N, forward unnormalised, inverse scaled by 1/N
+ * (the reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length.
+ * Powers of two from 16 to 2^38 (C64) / 2^35 (C128) run the fused passes: up
+ * to 2^26 (C64) / 2^24 (C128) a split step costs two passes over the field,
+ * beyond that four (three-level plans); log_rows + log_cols = log2 N. Other
+ * lengths from 1 to 2^31 (cufftPlan1d's int range) use Bluestein's algorithm
+ * on a power-of-two plan of length M >= 2N - 1 (a transform costs three of
+ * length M; log_rows = log_cols = 0), as do powers of two below 16. The
+ * length-M plan takes the tuning registered for M, if any.
  * The plan owns its twiddle tables and scratch; it is bound to the device that
  * is current at creation. */
 rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype);
@@ -89,7 +93,7 @@ typedef struct {
     int row_e, col_e, mid_e;
 } rsw_tuning;
 rsw_status rsw_plan_create_tuned(rsw_plan *out, int64_t n, int dtype, const rsw_tuning *tuning);
-/* The plan's effective choices. */
+/* The plan's effective choices (of its length-M plan for Bluestein lengths). */
 rsw_status rsw_plan_tuning(rsw_plan plan, rsw_tuning *tuning);
 /* Register the tuning that later rsw_plan_create / rsw_sim_create calls use
  * for this n and dtype (process-wide; tuning == NULL removes it). The

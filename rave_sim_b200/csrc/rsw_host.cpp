@@ -49,6 +49,12 @@ cudaError_t launch_detect(const void *u, const int64_t *bounds, const double *co
 cudaError_t launch_zero(double *p, int64_t n, cudaStream_t s);
 cudaError_t launch_fill_ones(void *u, int64_t n, bool dbl, cudaStream_t s);
 cudaError_t launch_chirp_table(void *out, int log_n2, double hi, double lo, bool dbl, int e, cudaStream_t s);
+cudaError_t launch_blue_pre(const void *in, void *w, int64_t n, int64_t m, const double2 *b, bool conj_in, bool dbl,
+                            cudaStream_t s);
+cudaError_t launch_blue_mul(void *w, const double2 *bh, int64_t m, bool dbl, cudaStream_t s);
+cudaError_t launch_blue_post(const void *w, void *out, int64_t n, const double2 *b, double scale, bool conj_out,
+                             bool dbl, cudaStream_t s);
+cudaError_t launch_prop_natural(void *U, int64_t n, const PropArgs &p, bool dbl, cudaStream_t s);
 unsigned long long launch_count();
 }  // namespace rsw
 
@@ -199,7 +205,10 @@ static rsw_status detector_geom(int64_t n, double dx, double det_size, double ps
     if (!(psx > 0) || !(det_size > 0)) return fail(RSW_ERR_INVALID, "detector size and pixel size must be positive");
     const double nf = py_floordiv(det_size, psx);
     const int64_t outsize = int64_t(nf);
-    if (outsize > n) return fail(RSW_ERR_INVALID, "detector has %lld pixels > N", (long long)outsize);
+    // more pixels than samples is allowed (the pixels no sample reaches stay 0,
+    // as in np.histogram); one CTA per pixel bounds the count by the grid
+    if (!(nf <= 2147483647.0))
+        return fail(RSW_ERR_UNSUPPORTED, "detector has %.0f pixels: at most 2^31 - 1", nf);
     g.n_pix = outsize;
     const double first = -(double(outsize) / 2.0) * psx;
     const double last = (double(outsize) / 2.0 + 1.0) * psx;
@@ -207,7 +216,7 @@ static rsw_status detector_geom(int64_t n, double dx, double det_size, double ps
     const double denom = last - first;
     const double step = denom / double(nb);
     auto edge = [&](int64_t i) { return i >= nb ? last : double(i) * step + first; };
-    auto pos = [&](int64_t i) { return (double(i) - double(n / 2)) * dx; };
+    auto pos = [&](int64_t i) { return (double(i) - double(n) / 2.0) * dx; };  // the reference's N / 2
     auto bin = [&](double a) -> int64_t {
         const double f = ((a - first) / denom) * double(nb);
         int64_t idx = int64_t(f);
@@ -321,6 +330,13 @@ struct rsw_plan_s {
     DevBuf chunk_xs, chunk_st;                            // per-call chunk tables
     DevBuf sample_grid, sample_db, sample_fac;            // per-call sample row data
     DevBuf h3_call;                                       // per-call chirp table
+    // lengths that are not a power of two (Bluestein): the power-of-two plan
+    // of length m >= 2n - 1, the chirp exp(i pi k^2 / n) (n entries, FP64), the
+    // FP64 spectrum of the extended chirp (m entries) and m samples of work space
+    bool blue = false;
+    std::unique_ptr<rsw_plan_s> inner;
+    int64_t m = 0;
+    DevBuf bchirp, bhat, bwork;
     bool dbl() const { return dtype == RSW_C128; }
     size_t elem() const { return dbl() ? 16 : 8; }
     bool three() const { return log_nb > 0; }
@@ -823,10 +839,14 @@ size_t rsw_struct_size(int which) {
     }
 }
 
+static rsw_status create_blue_plan(rsw_plan *out, int64_t n, int dtype);
+
 static rsw_status create_plan(rsw_plan *out, int64_t n, int dtype, const rsw_tuning *t) {
     if (!out) return fail(RSW_ERR_INVALID, "out is NULL");
     *out = nullptr;
     if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
+    // lengths that are not a power of two, and powers of two below 16
+    if (n >= 1 && ((n & (n - 1)) != 0 || n < 16)) return create_blue_plan(out, n, dtype);
     int lg, l1, lb, lr;
     CHECK(plan_split(n, dtype, &lg, &l1, &lb, &lr, t));
     std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
@@ -845,6 +865,86 @@ static rsw_status create_plan(rsw_plan *out, int64_t n, int dtype, const rsw_tun
     return RSW_OK;
 }
 
+// A plan for a length that is not a power of two (Bluestein's algorithm over
+// the power-of-two plan of length m >= 2n - 1). The extended chirp's spectrum
+// is taken once with an FP64 plan of length m, also for complex64 plans.
+static rsw_status create_blue_plan(rsw_plan *out, int64_t n, int dtype) {
+    if (n > (int64_t(1) << 31)) return fail(RSW_ERR_UNSUPPORTED, "lengths that are not a power of two: at most 2^31");
+    int64_t m = 16;
+    while (m < 2 * n - 1) m <<= 1;
+    std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
+    if (!p) return fail(RSW_ERR_NOMEM, "host allocation failed");
+    p->n = n;
+    p->dtype = dtype;
+    p->blue = true;
+    p->m = m;
+    CU(cudaGetDevice(&p->device));
+    rsw_plan inner = nullptr;
+    rsw_tuning reg{};
+    const bool use = !env_overrides() && registered_tuning(m, dtype, &reg);
+    CHECK(create_plan(&inner, m, dtype, use ? &reg : nullptr));
+    p->inner.reset(inner);
+    // chirp b[k] = exp(i pi k^2 / n), k^2 reduced mod 2n exactly
+    const long double pi = 3.14159265358979323846264338327950288L;
+    std::vector<double> b(size_t(2 * n)), bx(size_t(2 * m), 0.0);
+    for (int64_t k = 0; k < n; ++k) {
+        const uint64_t r = (uint64_t(k) * uint64_t(k)) % uint64_t(2 * n);
+        const long double ang = pi * (long double)r / (long double)n;
+        b[size_t(2 * k)] = double(cosl(ang));
+        b[size_t(2 * k + 1)] = double(sinl(ang));
+    }
+    // extended chirp: b[j] at j and at m - j
+    for (int64_t j = 0; j < n; ++j) {
+        bx[size_t(2 * j)] = b[size_t(2 * j)];
+        bx[size_t(2 * j + 1)] = b[size_t(2 * j + 1)];
+        if (j > 0) {
+            bx[size_t(2 * (m - j))] = b[size_t(2 * j)];
+            bx[size_t(2 * (m - j) + 1)] = b[size_t(2 * j + 1)];
+        }
+    }
+    CHECK(p->bchirp.upload(b));
+    CHECK(p->bhat.upload(bx));
+    rsw_plan p64 = inner;
+    std::unique_ptr<rsw_plan_s> own;
+    if (dtype != RSW_C128) {
+        CHECK(create_plan(&p64, m, RSW_C128, nullptr));
+        own.reset(p64);
+    }
+    CHECK(rsw_fft_forward(p64, p->bhat.p, p->bhat.p, nullptr));
+    CU(cudaDeviceSynchronize());  // the spectrum is complete before the temporary plan goes
+    CHECK(p->bwork.alloc(size_t(m) * p->elem()));
+    *out = p.release();
+    return RSW_OK;
+}
+
+// Natural-order DFT of a Bluestein plan (inverse: conj(DFT(conj X)) / n).
+static rsw_status blue_transform(rsw_plan_s *p, const void *in, void *out, bool inverse, cudaStream_t s) {
+    cudaError_t e = launch_blue_pre(in, p->bwork.p, p->n, p->m, (const double2 *)p->bchirp.p, inverse, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "bluestein: %s", cudaGetErrorString(e));
+    CHECK(rsw_fft_forward(p->inner.get(), p->bwork.p, p->bwork.p, s));
+    e = launch_blue_mul(p->bwork.p, (const double2 *)p->bhat.p, p->m, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "bluestein: %s", cudaGetErrorString(e));
+    CHECK(rsw_fft_inverse(p->inner.get(), p->bwork.p, p->bwork.p, s));
+    e = launch_blue_post(p->bwork.p, out, p->n, (const double2 *)p->bchirp.p, inverse ? 1.0 / double(p->n) : 1.0,
+                         inverse, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "bluestein: %s", cudaGetErrorString(e));
+    return RSW_OK;
+}
+
+// propagate() of a Bluestein plan: U = FFT(u) (unless given), transfer
+// function and cutoff on the natural-order spectrum, u = iFFT(U).
+static rsw_status blue_propagate(rsw_plan_s *p, void *u, void *U, const PropArgs &pr, bool skip_fft, cudaStream_t s) {
+    void *spec = U;
+    if (!spec) {
+        CHECK(p->scratch.alloc(size_t(p->n) * p->elem()));
+        spec = p->scratch.p;
+    }
+    if (!skip_fft) CHECK(blue_transform(p, u, spec, false, s));
+    cudaError_t e = launch_prop_natural(spec, p->n, pr, p->dbl(), s);
+    if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "transfer function: %s", cudaGetErrorString(e));
+    return blue_transform(p, spec, u, true, s);
+}
+
 rsw_status rsw_plan_create(rsw_plan *out, int64_t n, int dtype) {
     rsw_tuning reg{};
     const bool use = !env_overrides() && registered_tuning(n, dtype, &reg);
@@ -857,6 +957,7 @@ rsw_status rsw_plan_create_tuned(rsw_plan *out, int64_t n, int dtype, const rsw_
 
 rsw_status rsw_plan_tuning(rsw_plan p, rsw_tuning *t) {
     if (!p || !t) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (p->blue) return rsw_plan_tuning(p->inner.get(), t);  // the transforms of length m do the work
     t->levels = p->log_n1 == 0 ? 1 : p->three() ? 3 : 2;
     t->log_rows = p->log_n1;
     t->log_mid = p->log_nb;
@@ -1026,6 +1127,7 @@ static cudaError_t to_spec(const rsw_plan_s *p, const void *nat, void *spec, cud
 rsw_status rsw_fft_forward(rsw_plan p, const void *in, void *out, void *stream) {
     if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
     cudaStream_t s = (cudaStream_t)stream;
+    if (p->blue) return blue_transform(p, in, out, false, s);
     CHECK(need_scratch(p));
     PassArgs a = base_args(p);
     a.in = in;
@@ -1047,6 +1149,7 @@ rsw_status rsw_fft_forward(rsw_plan p, const void *in, void *out, void *stream) 
 rsw_status rsw_fft_inverse(rsw_plan p, const void *in, void *out, void *stream) {
     if (!p || !in || !out) return fail(RSW_ERR_INVALID, "NULL argument");
     cudaStream_t s = (cudaStream_t)stream;
+    if (p->blue) return blue_transform(p, in, out, true, s);
     CHECK(need_scratch(p));
     cudaError_t e = to_spec(p, in, p->scratch.p, s);
     if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "reorder: %s", cudaGetErrorString(e));
@@ -1211,6 +1314,7 @@ rsw_status rsw_propagate(rsw_plan p, void *u, void *U, double dx, double wl, dou
     cudaStream_t s = (cudaStream_t)stream;
     PassArgs a = base_args(p);
     a.pr = make_prop(p->n, dx, wl, dz, cutoff_freq, dz != 0.0, p->prop_mode == RSW_PROP_EXACT);
+    if (p->blue) return blue_propagate(p, u, U, a.pr, skip_fft != 0, s);
     const bool two = p->log_n1 > 0;
     if (two && a.pr.has_h && !a.pr.exact) {
         CHECK(p->h3_call.alloc(size_t(int64_t(1) << p->log_nr) * 16));  // 16-byte entries
@@ -1602,8 +1706,20 @@ struct Runner {
         CHECK(chirp_for(a.pr, dz));
         a.in = ones ? nullptr : bp(cur);
         a.out = bp(dst);
-        bool now_mid;
-        CHECK(launch_split_step(P, a, mid, ones, st, &S->tl, &now_mid));
+        bool now_mid = false;
+        if (P->blue) {
+            // any length: transmission and propagate on the natural-order field
+            void *d = bp(dst);
+            cudaError_t e = cudaSuccess;
+            if (ones) e = launch_fill_ones(d, P->n, P->dbl(), st);
+            else if (cur != dst)
+                e = cudaMemcpyAsync(d, bp(cur), size_t(P->n) * P->elem(), cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess && tr.kind != TR_NONE) e = launch_trans(d, P->n, tr, P->dbl(), st);
+            if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "split step: %s", cudaGetErrorString(e));
+            CHECK(blue_propagate(P, d, nullptr, a.pr, false, st));
+        } else {
+            CHECK(launch_split_step(P, a, mid, ones, st, &S->tl, &now_mid));
+        }
         if (commit) {
             cur = dst;
             ones = false;

@@ -67,7 +67,7 @@ template <typename Cx>
 __global__ void point_source_kernel(Cx *__restrict__ u, int64_t n, double dx, double w, double z,
                                     double x_src) {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    const double half = double(n / 2);
+    const double half = double(n) / 2.0;  // the reference's N / 2 (a float for odd N)
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const double x = __dsub_rn(__dmul_rn(double(i) - half, dx), x_src);
         const double r = sqrt(__dadd_rn(__dmul_rn(x, x), __dmul_rn(z, z)));
@@ -243,6 +243,111 @@ cudaError_t launch_zero(double *p, int64_t n, cudaStream_t s) {
     return cudaGetLastError();
 }
 unsigned long long launch_count() { return g_launches.load(); }
+
+// ------------------------------------------------------- Bluestein (any N)
+// A length-N DFT as a circular convolution of length M >= 2N - 1 (a power of
+// two), with the chirp b[k] = exp(i pi k^2 / N):
+//   X[k] = conj(b[k]) sum_j (x[j] conj(b[j])) b[k - j].
+// The pointwise products are taken in FP64 for both field types (the tables
+// are FP64), so the fields round once per product.
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(double(a.x), double(a.y)); }
+template <typename Cx>
+__global__ void blue_pre_kernel(const Cx *__restrict__ in, Cx *__restrict__ w, int64_t n, int64_t m,
+                                const double2 *__restrict__ b, int conj_in) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < m; k += stride) {
+        if (k < n) {
+            double2 x = to_d(in[k]);
+            if (conj_in) x.y = -x.y;
+            w[k] = to_c(cmulc(x, b[k]), Cx{});
+        } else {
+            w[k] = to_c(make_double2(0.0, 0.0), Cx{});
+        }
+    }
+}
+template <typename Cx>
+__global__ void blue_mul_kernel(Cx *__restrict__ w, const double2 *__restrict__ bh, int64_t m) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < m; k += stride)
+        w[k] = to_c(cmul(to_d(w[k]), bh[k]), Cx{});
+}
+template <typename Cx>
+__global__ void blue_post_kernel(const Cx *__restrict__ w, Cx *__restrict__ out, int64_t n,
+                                 const double2 *__restrict__ b, double scale, int conj_out) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride) {
+        double2 y = cmulc(to_d(w[k]), b[k]);
+        y = make_double2(y.x * scale, (conj_out ? -y.y : y.y) * scale);
+        out[k] = to_c(y, Cx{});
+    }
+}
+// Transfer function and cutoff on a natural-order spectrum of any length:
+// ks = k or k - N (np.fft.fftfreq's order), fx = (ks * (1/N)) / dx in the
+// reference's order (big-wave/propagation.py:154-175, :124-128), applied in FP64.
+template <typename Cx>
+__global__ void prop_natural_kernel(Cx *__restrict__ U, int64_t n, PropArgs p) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t pos_end = (n - 1) / 2 + 1;
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += stride) {
+        if (p.has_cut && k >= p.cut_lo && k < p.cut_hi) {
+            U[k] = to_c(make_double2(0.0, 0.0), Cx{});
+            continue;
+        }
+        if (!p.has_h) continue;
+        const int64_t ks = k < pos_end ? k : k - n;
+        const double fx = __ddiv_rn(__dmul_rn(double(ks), p.fac), p.dx);
+        double ph;
+        if (p.exact) {
+            const double f2 = __dmul_rn(fx, fx);
+            const double d = __dsub_rn(p.inv_wl2, f2);
+            if (!(d > 0.0)) {
+                U[k] = to_c(make_double2(0.0, 0.0), Cx{});
+                continue;
+            }
+            ph = __ddiv_rn(__dmul_rn(p.z2pi, f2), __dadd_rn(p.inv_wl, __dsqrt_rn(d)));
+        } else {
+            ph = __dmul_rn(p.c, __dmul_rn(fx, fx));
+        }
+        double sn, cs;
+        sincos_phase(ph, &sn, &cs);
+        const double2 H = make_double2(p.A.x * cs - p.A.y * sn, p.A.x * sn + p.A.y * cs);
+        U[k] = to_c(cmul(to_d(U[k]), H), Cx{});
+    }
+}
+
+cudaError_t launch_blue_pre(const void *in, void *w, int64_t n, int64_t m, const double2 *b, bool conj_in, bool dbl,
+                            cudaStream_t s) {
+    ++g_launches;
+    if (dbl)
+        blue_pre_kernel<double2><<<grid_for(m, 256), 256, 0, s>>>((const double2 *)in, (double2 *)w, n, m, b, conj_in);
+    else
+        blue_pre_kernel<float2><<<grid_for(m, 256), 256, 0, s>>>((const float2 *)in, (float2 *)w, n, m, b, conj_in);
+    return cudaGetLastError();
+}
+cudaError_t launch_blue_mul(void *w, const double2 *bh, int64_t m, bool dbl, cudaStream_t s) {
+    ++g_launches;
+    if (dbl) blue_mul_kernel<double2><<<grid_for(m, 256), 256, 0, s>>>((double2 *)w, bh, m);
+    else blue_mul_kernel<float2><<<grid_for(m, 256), 256, 0, s>>>((float2 *)w, bh, m);
+    return cudaGetLastError();
+}
+cudaError_t launch_blue_post(const void *w, void *out, int64_t n, const double2 *b, double scale, bool conj_out,
+                             bool dbl, cudaStream_t s) {
+    ++g_launches;
+    if (dbl)
+        blue_post_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((const double2 *)w, (double2 *)out, n, b, scale,
+                                                                  conj_out);
+    else
+        blue_post_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((const float2 *)w, (float2 *)out, n, b, scale,
+                                                                 conj_out);
+    return cudaGetLastError();
+}
+cudaError_t launch_prop_natural(void *U, int64_t n, const PropArgs &p, bool dbl, cudaStream_t s) {
+    ++g_launches;
+    if (dbl) prop_natural_kernel<double2><<<grid_for(n, 256), 256, 0, s>>>((double2 *)U, n, p);
+    else prop_natural_kernel<float2><<<grid_for(n, 256), 256, 0, s>>>((float2 *)U, n, p);
+    return cudaGetLastError();
+}
 
 }  // namespace rsw
 

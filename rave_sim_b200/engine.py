@@ -93,7 +93,8 @@ def _pair(c: complex):
 
 
 class Plan:
-    """FFT plan of length ``n`` (a power of two) for c16 or c8 fields."""
+    """FFT plan of length ``n`` for c16 or c8 fields (any n >= 1: powers of two
+    >= 16 run the pass kernels, other lengths Bluestein's algorithm over them)."""
 
     def __init__(self, n: int, dtype="c16", tuning: Optional[dict] = None):
         """``tuning``: explicit schedule choices (rave_sim_b200.autotune.FIELDS;

@@ -288,6 +288,56 @@ def _cases():
     c8["history_dz"] = 0.013
     cases.append(c8)
 
+    # 9. big-wave's own test_stepping setup (big-wave/test.py:251-300): N = 6,
+    #    a point source, two vacuum gratings (the second phase-stepped),
+    #    cutoff angles 0.1 / 0.2 / 0.3, history every 0.1 m.
+    def _vacuum_grating(z, xs):
+        return {"type": "grating", "pitch": 4.2e-6, "dc": [0.5, 0.5], "z_start": z, "thickness": 100e-6,
+                "nr_steps": 1, "x_positions": xs, "substrate_thickness": 0.0, "mat_a": None, "mat_b": None,
+                "mat_substrate": None}
+    cases.append(dict(
+        name="stepping_n6",
+        sim_params=dict(N=6, dx=10e-9, z_detector=1.0, detector_size=40e-9, detector_pixel_size_x=20e-9,
+                        detector_pixel_size_y=1.0, chunk_size=3),
+        elements=[_vacuum_grating(0.1, [0.0]), _vacuum_grating(0.2, [0.0, 1.6e-6, 3.1e-6])],
+        source=dict(type="point", x=0.0, z=0.0), energy=46000.0, db=[],
+        cutoff_angles=[0.1, 0.2, 0.3], history_dz=0.1, save_u=False,
+    ))
+
+    # 10. an odd length (3^8): point source off axis, a chunked grating, a
+    #     pixelised sample, active cutoffs (the reference's N / 2 and N // 2
+    #     conventions differ for odd N).
+    N = 3 ** 8
+    grid10 = np.random.default_rng(11).integers(0, 3, size=(5, 29)).astype(np.int8)
+    cases.append(dict(
+        name="odd_point_sample",
+        sim_params=dict(N=N, dx=2e-9, z_detector=0.12, detector_size=10e-6, detector_pixel_size_x=0.5e-6,
+                        detector_pixel_size_y=1.0, chunk_size=1000),
+        elements=[
+            _grating(0.02, 1.9e-6, 20e-6, 2, [0.0], SI, None),
+            {"type": "sample", "z_start": 0.05, "pixel_size_x": 0.35e-6, "pixel_size_z": 4e-6,
+             "grid_path": "grid.npy", "materials": [AL, SI], "x_positions": [0.0]},
+        ],
+        grid=grid10,
+        source=dict(type="point", x=0.05e-6, z=0.0), energy=35000.0,
+        db=[[AL, [4.4e-7, 2e-9]], [SI, [4.0e-7, 1e-9]]],
+        cutoff_angles=[5e-5, 6e-5, 7e-5],
+        save_u=False,
+    ))
+
+    # 11. an even length that is not a power of two: plane wave, a grating
+    #     stepped over 3 positions, then a gap.
+    N = 12000
+    cases.append(dict(
+        name="nonpow2_plane",
+        sim_params=dict(N=N, dx=1e-9, z_detector=0.08, detector_size=10e-6, detector_pixel_size_x=1e-6,
+                        detector_pixel_size_y=1.0, chunk_size=N),
+        elements=[_grating(0.02, 2e-6, 30e-6, 3, [0.0, 0.5e-6, 1.0e-6], SI, None)],
+        source=dict(type="plane", z=0.02), energy=46000.0,
+        db=[[SI, [2.27e-7, 1e-10]]], cutoff_angles=[np.pi / 2] * 2,
+        save_u=True,
+    ))
+
     return cases
 
 

@@ -39,7 +39,10 @@ def test_struct_layouts():
 def test_invalid_sizes_rejected_without_device():
     lib = L.load()
     h = C.c_void_p()
-    for n, code in [(6, L.RSW_ERR_UNSUPPORTED), (1000, L.RSW_ERR_UNSUPPORTED), (8, L.RSW_ERR_UNSUPPORTED),
+    # any length from 1 to 2^31 is planned (Bluestein's algorithm where it is
+    # not a power of two >= 16); these are refused before any device call
+    for n, code in [(0, L.RSW_ERR_UNSUPPORTED), (-6, L.RSW_ERR_UNSUPPORTED),
+                    ((1 << 31) + 1, L.RSW_ERR_UNSUPPORTED), (3 << 31, L.RSW_ERR_UNSUPPORTED),
                     (1 << 40, L.RSW_ERR_UNSUPPORTED)]:
         st = lib.rsw_plan_create(C.byref(h), n, L.RSW_C128)
         assert st == code, (n, st)

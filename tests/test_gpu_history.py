@@ -18,7 +18,8 @@ import rave_sim_b200 as rsw  # noqa: E402
 NAMES = ["hist_point_tl", "hist_sample"]
 
 
-@pytest.mark.parametrize("name", NAMES)
+# stepping_n6: big-wave's test_stepping setup at N = 6 (a Bluestein plan)
+@pytest.mark.parametrize("name", NAMES + ["stepping_n6"])
 @pytest.mark.parametrize("dtype,tol", [("c16", 1e-10), ("c8", 1e-5)])
 def test_history_matches_reference(name, dtype, tol):
     case, grids, d = load_case(name)

@@ -236,7 +236,11 @@ def test_config1_full_size():
 
 def test_errors_are_raised():
     with pytest.raises(rsw.RswError):
-        rsw.Plan(1000, "c16")
+        rsw.Plan(0, "c16")
+    with pytest.raises(rsw.RswError):
+        rsw.Plan((1 << 31) + 1, "c16")  # Bluestein lengths end at 2^31
+    with pytest.raises(ValueError):
+        rsw.Plan(1 << 10, "c16").set_propagator("angular")
     p = rsw.Plan(1 << 10, "c16")
     with pytest.raises(ValueError):
         p.fft(torch.zeros(10, dtype=torch.complex128, device=DEV))

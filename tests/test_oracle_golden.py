@@ -79,7 +79,7 @@ def test_energy_conversion():
     assert abs(bw.wavelength_from_energy(46000) - 26.95e-12) < 0.01e-12
 
 
-@pytest.mark.parametrize("name", ["hist_point_tl", "hist_sample"])
+@pytest.mark.parametrize("name", ["hist_point_tl", "hist_sample", "stepping_n6"])
 def test_oracle_history_matches_reference(name):
     """History recording (big-wave/history.py) against the reference's own
     History of the same run."""
