@@ -341,6 +341,16 @@ rsw_status rsw_sim_set_history(rsw_sim sim, double history_dz);
 rsw_status rsw_sim_set_propagator(rsw_sim sim, int mode);
 rsw_status rsw_sim_history(rsw_sim sim, double *h_history, double *h_z, int64_t *n_entries,
                            void *stream);
+/* Keypoints (replaces big-wave's save_keypoints_path, wavesim.py:35-55,
+ * :186, :196): during the first phase-step pass of each following run, the
+ * field in natural order right before element i is written to dst[2 i] and
+ * right after it (grating sub-steps or sample slices done) to dst[2 i + 1].
+ * dst holds n_dst = 2 * n_elements device buffers of N samples of the
+ * simulation's dtype on its device (NULL entries are skipped); the pointers
+ * are kept until the next call, and n_dst = 0 turns keypoints off. Each
+ * keypoint costs one copy, or one inverse column pass where the field is held
+ * in the passes' intermediate order. */
+rsw_status rsw_sim_set_keypoints(rsw_sim sim, void *const *dst, int64_t n_dst);
 
 #ifdef __cplusplus
 }

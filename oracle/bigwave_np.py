@@ -355,7 +355,7 @@ def analytic_history(hist, zs, x_source, sim, cutoff):
         hist.append((inten, z))
 
 
-def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False, history_dz=None):
+def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False, history_dz=None, keypoints=None):
     """``run_simulation`` (big-wave/wavesim.py:84-298) for one source: source
     initialisation, element loop with gap propagation, final gap reusing the
     spectrum (``skip_fft``), detection, then the remaining phase steps
@@ -365,7 +365,10 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False, h
     Returns the detector array ``(nr_phase_steps, n_pix)`` (and the final
     fields of every phase step when ``return_fields``). With ``history_dz``
     the first pass records the history (big-wave/wavesim.py:153-219) and the
-    result is ``(detector, history (n_pix, entries), z of each entry)``."""
+    result is ``(detector, history (n_pix, entries), z of each entry)``.
+    A ``keypoints`` list receives copies of the field right before and right
+    after each element of the first pass (big-wave/wavesim.py:35-55, :186,
+    :196), in element order."""
     hist = [] if history_dz else None
     grids = grids or {}
     sim = make_sim(case)
@@ -416,7 +419,11 @@ def run_simulation(case, grids=None, dtype=np.complex128, return_fields=False, h
         if len(el["x_positions"]) > 1 and snapshot is None:
             snapshot = (z, i, u.copy(), len(el["x_positions"]))
         cutoff = cut[i + 1]
+        if keypoints is not None:
+            keypoints.append(u.copy())
         u, U = apply(el, u, U, cutoff, 0, hist)
+        if keypoints is not None:
+            keypoints.append(u.copy())
         z = el["z_start"] + element_thickness(el)
     if z < sim.z_detector - z_tol:
         u, U = propagate_with_history(u, U, sim, sim.z_detector - z, cutoff, z, len(elements) > 0, hist,

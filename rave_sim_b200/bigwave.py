@@ -12,14 +12,15 @@ tests can run on the engine unchanged:
     run_simulation(params, source, elements, cutoff_angles, u, U,
                    deltabeta_table, sub_dir, vectors_dir, save_final_u_vectors,
                    history=None, save_keypoints_path=None) -> list[np.ndarray]
-        big-wave/wavesim.py:84-298 (history and keypoints are not supported:
-        they record intermediate fields, which the fused engine never forms)
+        big-wave/wavesim.py:84-298, with history and keypoints (the field
+        before and after each element, saved as keypoint_{el:02}_{0|1}.npy)
 
 Errors are raised as ``ValueError`` / ``AssertionError`` like the reference's.
 """
 
 from __future__ import annotations
 
+from pathlib import Path
 from typing import Optional
 
 import numpy as np
@@ -105,8 +106,6 @@ def run_simulation(params, source, elements, cutoff_angles, u, U, deltabeta_tabl
     in ``u``. ``history`` is big-wave's ``(History, dz)`` pair
     (big-wave/wavesim.py:95, :129-131): the engine records the history and its
     entries are pushed into the History object in order."""
-    if save_keypoints_path is not None:
-        raise ValueError("keypoints are not supported by the fused engine")
     n = len(u)
     dtype = u.vec.dtype
     config = {
@@ -133,8 +132,15 @@ def run_simulation(params, source, elements, cutoff_angles, u, U, deltabeta_tabl
         sim.reset()
         if history is not None:
             sim.set_history(float(history[1]))
+        if save_keypoints_path is not None:
+            sim.set_keypoints(True)
         sim.run_source(energy=1.0, wavelength=float(params.wl), db_table=table, source=src, field=field)
         det = sim.detected()
+        if save_keypoints_path is not None:
+            # save_keypoint (big-wave/wavesim.py:35-55)
+            kp_dir = Path(save_keypoints_path)
+            for k, t in enumerate(sim.keypoints()):
+                np.save(kp_dir / f"keypoint_{k // 2:02}_{k % 2}.npy", t.cpu().numpy())
         if history is not None:
             images, zs = sim.history()
             for e in range(images.shape[1]):

@@ -1629,6 +1629,9 @@ struct rsw_sim_s {
     DevBuf hist, hist_cos, hist_r;
     int64_t hist_cap = 0;
     std::vector<double> hist_z;
+    // keypoints (big-wave/wavesim.py:35-55): caller buffers for the field
+    // before / after each element of the first pass, NULL entries skipped
+    std::vector<void *> keypoints;
     ~rsw_sim_s() { rsw_plan_destroy(plan); }
 };
 
@@ -1813,6 +1816,26 @@ struct Runner {
         }
         CHECK(split_step(TransArgs{}, zs.back() - zs[0], cutoff));
         return hist_push(zs.back() + z_from);
+    }
+
+    // save_keypoint (big-wave/wavesim.py:35-55): the current field in natural
+    // order into a caller buffer; the state is left as it is
+    rsw_status keypoint(void *dst) {
+        if (!dst) return RSW_OK;
+        cudaError_t e = cudaSuccess;
+        if (ones) {
+            e = launch_fill_ones(dst, P->n, P->dbl(), st);
+        } else if (mid) {
+            PassArgs a = base_args(P);
+            a.in = bp(cur);
+            a.out = dst;
+            a.flags = col_inv(P);
+            return run_col(P, a, st);
+        } else {
+            e = cudaMemcpyAsync(dst, bp(cur), size_t(P->n) * P->elem(), cudaMemcpyDeviceToDevice, st);
+        }
+        if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "keypoint: %s", cudaGetErrorString(e));
+        return RSW_OK;
     }
 
     rsw_status finalize() {
@@ -2135,6 +2158,19 @@ rsw_status rsw_sim_set_history(rsw_sim S, double history_dz) {
     return RSW_OK;
 }
 
+rsw_status rsw_sim_set_keypoints(rsw_sim S, void *const *dst, int64_t n_dst) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    if (n_dst == 0) {
+        S->keypoints.clear();
+        return RSW_OK;
+    }
+    if (!dst || n_dst != 2 * int64_t(S->els.size()))
+        return fail(RSW_ERR_INVALID, "keypoints: %lld buffers for %zu elements (2 per element)", (long long)n_dst,
+                    S->els.size());
+    S->keypoints.assign(dst, dst + n_dst);
+    return RSW_OK;
+}
+
 rsw_status rsw_sim_history(rsw_sim S, double *h_out, double *h_z, int64_t *n_entries, void *stream) {
     if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
     const int64_t n = int64_t(S->hist_z.size()), np = S->geom.n_pix;
@@ -2265,7 +2301,10 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
             R.readonly = R.cur;
         }
         cutoff = R.cut[i + 1];
+        const bool kp = s.keypoints.size() == size_t(2 * nel);
+        if (kp) CHECK(R.keypoint(s.keypoints[size_t(2 * i)]));
         CHECK(R.apply(i, 0, cutoff));
+        if (kp) CHECK(R.keypoint(s.keypoints[size_t(2 * i + 1)]));
         z = e.z_start + s.els[i].total_thickness();
     }
     if (z < s.d.z_detector - z_tol) CHECK(R.gap(s.d.z_detector - z, cutoff, z));

@@ -437,25 +437,53 @@ class Simulation:
                                           C.byref(n), _stream_ptr()))
         return h, z
 
+    def set_keypoints(self, enable: bool):
+        """Keep the field right before and right after each element of the
+        first pass of the following runs (big-wave's save_keypoints_path,
+        wavesim.py:35-55) in device buffers; ``keypoints()`` returns them."""
+        if not enable:
+            L.check(self._lib.rsw_sim_set_keypoints(self._h, None, 0))
+            self._kp = None
+            return
+        torch = _torch()
+        k = 2 * len(self.config["elements"])
+        bufs = [torch.empty(self.n, dtype=torch_dtype(self.code), device="cuda") for _ in range(k)]
+        ptrs = (C.c_void_p * max(k, 1))(*[_dptr(b) for b in bufs])
+        L.check(self._lib.rsw_sim_set_keypoints(self._h, ptrs, k))
+        self._kp = bufs
+
+    def keypoints(self):
+        """Keypoints of the last run, in big-wave's order (element 0 before,
+        element 0 after, element 1 before, ...): CUDA tensors of N samples."""
+        if getattr(self, "_kp", None) is None:
+            raise ValueError("keypoints are off (set_keypoints(True) before the run)")
+        return list(self._kp)
+
     def timing(self, kind: int):
         ms, n = C.c_double(), C.c_int64()
         L.check(self._lib.rsw_sim_timing(self._h, int(kind), C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
 
-def run_case(case: dict, grids: Optional[dict] = None, dtype=None, history_dz: Optional[float] = None):
+def run_case(case: dict, grids: Optional[dict] = None, dtype=None, history_dz: Optional[float] = None,
+             keypoints: Optional[list] = None):
     """Run one source described by a case dict (the oracle's schema: the
     reference config + ``source``, ``energy``, ``db``, ``cutoff_angles``) and
     return its detector array (nr_phase_steps, n_pix); with ``history_dz``,
-    (detector, history (n_pix, entries), z of each entry)."""
+    (detector, history (n_pix, entries), z of each entry). A ``keypoints``
+    list receives the keypoint fields as numpy arrays."""
     sim = Simulation(case, grids=grids, dtype=dtype if dtype is not None else case.get("dtype", "c16"),
                      cutoff_angles=case["cutoff_angles"])
     try:
         sim.set_history(history_dz)
+        if keypoints is not None:
+            sim.set_keypoints(True)
         sim.reset()
         sim.run_source(energy=case["energy"], db_table=case["db"], source=case["source"],
                        field=case["source"].get("u"))
         det = sim.detected()
+        if keypoints is not None:
+            keypoints.extend(t.cpu().numpy() for t in sim.keypoints())
         if history_dz:
             h, z = sim.history()
             return det, h, z

@@ -16,12 +16,14 @@ phase stepping, ``NNNNNNNN/u_0000.npy``. The command line mirrors fast-wave's
 ``fastwave <sim_dir> -s <idx>`` (fast-wave/main.cpp:18-57):
 
     python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16] [--history_dz DZ]
+        [--save_keypoints_path DIR]
 
 With ``--history_dz`` the history of the source is written as
 ``history.npy`` (n_pix, entries), ``history_z.npy`` and ``history_x.npy``
 (big-wave/multisim.py:132-141). The field stays in GPU memory for the whole
-source, so ``use_disk_vector`` is accepted and ignored. Keypoints are not
-supported.
+source, so ``use_disk_vector`` is accepted and ignored. With
+``--save_keypoints_path`` the field before and after each element of the first
+pass is written as ``keypoint_{element:02}_{0|1}.npy`` (big-wave/wavesim.py:35-55).
 """
 
 from __future__ import annotations
@@ -104,10 +106,14 @@ def load_source(sim_dir, source_idx: int) -> dict:
     }
 
 
-def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, dtype: Optional[str] = None,
-                          history_dz: Optional[float] = None) -> np.ndarray:
+def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, save_keypoints_path=None,
+                          history_dz: Optional[float] = None, dtype: Optional[str] = None) -> np.ndarray:
     """Run source ``source_idx`` of ``sim_dir`` and write its detected.npy
-    (big-wave/multisim.py:50-150). Returns the detector array."""
+    (big-wave/multisim.py:50-150, same argument order). With
+    ``save_keypoints_path`` the field before and after each element of the
+    first pass is saved there as keypoint_{element:02}_{0|1}.npy
+    (big-wave/wavesim.py:35-55). ``dtype`` overrides the config's. Returns the
+    detector array."""
     from .engine import Simulation
 
     sim_dir = Path(sim_dir)
@@ -122,9 +128,15 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, dtype: Opt
     sim = Simulation(c, grids=c["grids"], dtype=dt, cutoff_angles=c["cutoff_angles"])
     try:
         sim.set_history(history_dz)
+        if save_keypoints_path is not None:
+            sim.set_keypoints(True)
         sim.reset()
         sim.run_source(energy=c["energy"], db_table=c["db"], source=c["source"], field=field)
         det = sim.detected()
+        if save_keypoints_path is not None:
+            kp_dir = Path(save_keypoints_path)
+            for k, t in enumerate(sim.keypoints()):
+                np.save(kp_dir / f"keypoint_{k // 2:02}_{k % 2}.npy", t.cpu().numpy())
         out_dir = sub_dir(sim_dir, source_idx)
         if history_dz:
             h, z = sim.history()
@@ -150,9 +162,12 @@ def main(argv=None) -> int:
     ap.add_argument("-s", "--source_idx", type=int, required=True)
     ap.add_argument("--dtype", choices=["c8", "c16"], default=None, help="override the config's dtype")
     ap.add_argument("--history_dz", type=float, default=None)
+    ap.add_argument("--save_keypoints_path", default=None,
+                    help="directory for keypoint_{element:02}_{0|1}.npy (the field before / after each element)")
     a = ap.parse_args(argv)
     try:
-        run_single_simulation(a.sim_dir, a.source_idx, dtype=a.dtype, history_dz=a.history_dz)
+        run_single_simulation(a.sim_dir, a.source_idx, save_keypoints_path=a.save_keypoints_path,
+                              history_dz=a.history_dz, dtype=a.dtype)
     except Exception as e:  # mirror fastwave: message and non-zero exit, no traceback
         print(f"error: {e}", file=sys.stderr)
         return 1

@@ -272,6 +272,7 @@ def _cases():
     c6["source"] = dict(type="point", x=-0.1e-6, z=0.0)
     c6["cutoff_angles"] = [3e-5, 3e-5, 4e-5, 4e-5]
     c6["sim_params"]["chunk_size"] = 5000
+    c6["keypoints"] = True  # big-wave/wavesim.py:35-55: u before / after each element
     cases.append(c6)
 
     # 7./8. history recording (big-wave/history.py:43-135): a point source
@@ -286,6 +287,7 @@ def _cases():
     c8["name"] = "hist_sample"
     c8["grid"] = grid
     c8["history_dz"] = 0.013
+    c8["keypoints"] = True
     cases.append(c8)
 
     # 9. big-wave's own test_stepping setup (big-wave/test.py:251-300): N = 6,
@@ -301,7 +303,7 @@ def _cases():
                         detector_pixel_size_y=1.0, chunk_size=3),
         elements=[_vacuum_grating(0.1, [0.0]), _vacuum_grating(0.2, [0.0, 1.6e-6, 3.1e-6])],
         source=dict(type="point", x=0.0, z=0.0), energy=46000.0, db=[],
-        cutoff_angles=[0.1, 0.2, 0.3], history_dz=0.1, save_u=False,
+        cutoff_angles=[0.1, 0.2, 0.3], history_dz=0.1, save_u=False, keypoints=True,
     ))
 
     # 10. an odd length (3^8): point source off axis, a chunked grating, a
@@ -322,7 +324,7 @@ def _cases():
         source=dict(type="point", x=0.05e-6, z=0.0), energy=35000.0,
         db=[[AL, [4.4e-7, 2e-9]], [SI, [4.0e-7, 1e-9]]],
         cutoff_angles=[5e-5, 6e-5, 7e-5],
-        save_u=False,
+        save_u=False, keypoints=True,
     ))
 
     # 11. an even length that is not a power of two: plane wave, a grating
@@ -388,11 +390,26 @@ def _run_case(case, mods, tmp: Path):
     if case.get("history_dz"):
         import history as bw_history
         hist = (bw_history.History(), float(case["history_dz"]))
+    kp_dir = None
+    if case.get("keypoints"):
+        kp_dir = tmp / "keypoints"
+        kp_dir.mkdir(exist_ok=True)
     det = wavesim.run_simulation(
         params, s, elements, list(case["cutoff_angles"]), u, U, db_table,
         sub, sub, bool(case.get("save_u", False)), history=hist,
+        save_keypoints_path=kp_dir,
     )
     out = {"detected": np.array(det)}
+    if kp_dir is not None:
+        # keypoint_{element:02}_{0 before | 1 after}.npy, in element order;
+        # every s-th sample (s = N // 1024 at most) plus full-vector sums
+        kps = np.stack([np.load(kp_dir / f"keypoint_{i:02}_{k}.npy")
+                        for i in range(len(elements)) for k in (0, 1)])
+        stride = max(1, N // 1024)
+        out["keypoints_stride"] = np.int64(stride)
+        out["keypoints_sub"] = kps[:, ::stride]
+        out["keypoints_sum"] = kps.sum(axis=1)
+        out["keypoints_norm2"] = (np.abs(kps) ** 2).sum(axis=1)
     if hist is not None:
         out["history"] = hist[0].get_history()
         out["history_z"] = np.array(hist[0].get_z(), dtype=np.float64)

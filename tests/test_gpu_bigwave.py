@@ -135,3 +135,15 @@ def test_propagate_and_detect_shims():
                        detector_pixel_size_y=1e-6, wl=2.7e-11, chunk_size=n)
     det = bigwave.square_and_downsample(u, params, 0.3)
     assert rel_l2(det, bw.square_and_downsample(u.vec, sim, 0.3)) < 1e-13
+
+
+def test_run_simulation_shim_keypoints(tmp_path):
+    # save_keypoints_path (big-wave/wavesim.py:35-55): keypoint_{el:02}_{0|1}.npy
+    case, grids, d = load_case("stepping_n6")
+    params, src, els, table, u, U = _shim_inputs(case)
+    out = bigwave.run_simulation(params, src, els, case["cutoff_angles"], u, U, table, ".", ".", False,
+                                 save_keypoints_path=tmp_path)
+    assert rel_l2(np.array(out), d["detected"]) < 1e-10
+    kps = np.stack([np.load(tmp_path / f"keypoint_{i:02}_{k}.npy") for i in range(len(els)) for k in (0, 1)])
+    assert kps.dtype == np.complex128
+    assert rel_l2(kps[:, ::int(d["keypoints_stride"])], d["keypoints_sub"]) < 1e-10

@@ -103,3 +103,19 @@ def test_angular_kernel_reduces_to_fresnel_at_small_frequencies():
     pred = 2 * np.pi * dz * wl ** 3 * fx ** 4 / 8
     np.testing.assert_allclose(d[small], pred[small], rtol=1e-3, atol=1e-9)
     assert np.all(np.abs(np.abs(ha) - 1) < 1e-14)
+
+
+@pytest.mark.parametrize("name", ["sample_stepped", "hist_sample", "stepping_n6", "odd_point_sample"])
+def test_oracle_keypoints_match_reference(name):
+    """Keypoints (big-wave/wavesim.py:35-55): the field before and after each
+    element of the first pass, against the reference's own keypoint files
+    (every s-th sample and full-vector sums)."""
+    case, grids, d = load_case(name)
+    kps = []
+    bw.run_simulation(case, grids, keypoints=kps)
+    kps = np.stack(kps)
+    s = int(d["keypoints_stride"])
+    assert kps.shape[0] == d["keypoints_sub"].shape[0] == 2 * len(case["elements"])
+    assert rel_l2(kps[:, ::s], d["keypoints_sub"]) < 1e-13
+    assert rel_l2(kps.sum(axis=1), d["keypoints_sum"]) < 1e-12
+    assert rel_l2((np.abs(kps) ** 2).sum(axis=1), d["keypoints_norm2"]) < 1e-13
