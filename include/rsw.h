@@ -65,7 +65,7 @@ double rsw_energy_to_wavelength(double energy_ev);
  * a 1-D complex FFT of length N, forward unnormalised, inverse scaled by 1/N
  * (the reference's inverse + scale kernel, fft.cpp:34-44). 64-bit length.
  * Powers of two from 16 to 2^38 (C64) / 2^35 (C128) run the fused passes: up
- * to 2^26 (C64) / 2^24 (C128) a split step costs two passes over the field,
+ * to 2^26 (C64) / 2^25 (C128) a split step costs two passes over the field,
  * beyond that four (three-level plans); log_rows + log_cols = log2 N. Other
  * lengths from 1 to 2^31 (cufftPlan1d's int range) use Bluestein's algorithm
  * on a power-of-two plan of length M >= 2N - 1 (a transform costs three of

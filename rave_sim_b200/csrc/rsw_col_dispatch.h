@@ -24,6 +24,8 @@ template <bool DET> cudaError_t col_dispatch(const PassArgs &a, bool dbl, int e,
             RSW_COL_CASE16(double, 7)
             case 8: return e == 8 ? col_impl<double, 8, 16, 8, DET>(a, s) : col_impl<double, 8, 16, 16, DET>(a, s);
             RSW_COL_CASE_E(double, 9, 8, 8) RSW_COL_CASE_E(double, 10, 4, 4) RSW_COL_CASE_E(double, 11, 4, 4)
+            // 2^12 (tunings only): two columns per CTA, 32-byte row segments
+            case 12: return e == 8 ? col_impl<double, 12, 2, 8, DET>(a, s) : col_impl<double, 12, 2, 16, DET>(a, s);
         default: return cudaErrorInvalidValue;
         }
     }

@@ -309,6 +309,10 @@ struct DevBuf {
 
 // -------------------------------------------------------------------- plan
 static constexpr int ROW_MAX_C128 = 13, COL_MAX_C128 = 11;
+// complex128 columns of 2^12 (two-column tiles): two-level plans only, for
+// 2^25 (built in: 1.05 ms per split step against 1.31 ms for three levels)
+// and for tunings
+static constexpr int COL_TUNE_MAX_C128 = 12;
 static constexpr int ROW_MAX_C64 = 14, COL_MAX_C64 = 12;
 static std::atomic<uint64_t> g_api_calls{0};
 
@@ -459,7 +463,8 @@ static rsw_status tuned_split(int lg, int dtype, const rsw_tuning &t, int *l1, i
         return RSW_OK;
     }
     const int a = t.log_rows, b = t.levels == 3 ? t.log_mid : 0, c = lg - a - b;
-    if (a < 4 || a > col_max || (t.levels == 3 && (b < 4 || b > col_max)) || c < 7 || c > row_max ||
+    const int a_max = t.levels == 2 && dtype == RSW_C128 ? COL_TUNE_MAX_C128 : col_max;
+    if (a < 4 || a > a_max || (t.levels == 3 && (b < 4 || b > col_max)) || c < 7 || c > row_max ||
         (t.levels != 2 && t.levels != 3))
         return fail(RSW_ERR_INVALID, "tuning: split %d levels, %d / %d / %d of 2^%d is not available", t.levels, a, b,
                     c, lg);
@@ -507,7 +512,8 @@ static rsw_status plan_split(int64_t n, int dtype, int *log_n, int *l1, int *lb,
         *lr = lg;
         return RSW_OK;
     }
-    if (lg > row_max + col_max) {
+    const int col2 = dtype == RSW_C128 ? COL_TUNE_MAX_C128 : col_max;  // two-level column limit
+    if (lg > row_max + col2) {
         if (lg > row_max + 2 * col_max)
             return fail(RSW_ERR_UNSUPPORTED, "N = 2^%d exceeds the three-level limit 2^%d for this dtype", lg,
                         row_max + 2 * col_max);
@@ -566,7 +572,8 @@ static bool row_e_ok(int log_nr, bool multi, int e) {
     if (!multi) return e == 16;
     return (e == 16 && log_nr >= 7) || (e == 32 && log_nr >= 9) || (e == 8 && log_nr >= 11 && log_nr <= 13);
 }
-static bool col_e_ok(int log_l, int e) {
+static bool col_e_ok(int log_l, int e, bool c128) {
+    if (c128 && log_l == 12) return e == 8 || e == 16;
     return (e == 16 && log_l >= 4) || (e == 8 && log_l >= 8 && log_l <= 11) || (e == 32 && log_l >= 9);
 }
 
@@ -575,17 +582,17 @@ static rsw_status choose_tuning(rsw_plan_s *p, const rsw_tuning *t) {
     p->row_e = pick(p->log_nr, 16);
     const bool c128 = p->dtype == RSW_C128;
     const int l1 = p->log_n1;
-    p->col_e = (c128 && l1 >= 8 && l1 <= 11) || (!c128 && (l1 == 9 || (l1 == 10 && p->log_nb == 0))) ? 8 : pick(l1, 16);
+    p->col_e = (c128 && l1 >= 8 && l1 <= 12) || (!c128 && (l1 == 9 || (l1 == 10 && p->log_nb == 0))) ? 8 : pick(l1, 16);
     p->mid_e = pick(p->log_nb, 16);
     if (t) {
         const bool multi = p->log_n1 > 0;
         if (t->row_e && !row_e_ok(p->log_nr, multi, t->row_e))
             return fail(RSW_ERR_INVALID, "tuning: rows of 2^%d have no kernel with %d samples per thread", p->log_nr,
                         t->row_e);
-        if (t->col_e && (!multi || !col_e_ok(p->log_n1, t->col_e)))
+        if (t->col_e && (!multi || !col_e_ok(p->log_n1, t->col_e, c128)))
             return fail(RSW_ERR_INVALID, "tuning: no column kernel of 2^%d with %d samples per thread", p->log_n1,
                         t->col_e);
-        if (t->mid_e && (!p->three() || !col_e_ok(p->log_nb, t->mid_e)))
+        if (t->mid_e && (!p->three() || !col_e_ok(p->log_nb, t->mid_e, c128)))
             return fail(RSW_ERR_INVALID, "tuning: no middle kernel of 2^%d with %d samples per thread", p->log_nb,
                         t->mid_e);
         if (t->row_e) p->row_e = t->row_e;
@@ -995,15 +1002,19 @@ rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double
     const int col_max = dtype == RSW_C128 ? COL_MAX_C128 : COL_MAX_C64;
     std::vector<rsw_tuning> cands;
     if (lg <= row_max) cands.push_back(rsw_tuning{1, 0, 0, 16, 0, 0});
-    if (lg <= row_max + col_max) {
-        for (int l1 = 4; l1 <= col_max; ++l1) {
+    const bool c128 = dtype == RSW_C128;
+    const int col_tune = c128 ? COL_TUNE_MAX_C128 : col_max;
+    if (lg <= row_max + col_tune) {
+        for (int l1 = 4; l1 <= col_tune; ++l1) {
             const int lr = lg - l1;
             if (lr < 7 || lr > row_max) continue;
             for (int re : {16, 32, 8})
                 for (int ce : {16, 8, 32})
-                    if (row_e_ok(lr, true, re) && col_e_ok(l1, ce)) cands.push_back(rsw_tuning{2, l1, 0, re, ce, 0});
+                    if (row_e_ok(lr, true, re) && col_e_ok(l1, ce, c128))
+                        cands.push_back(rsw_tuning{2, l1, 0, re, ce, 0});
         }
-    } else {
+    }
+    if (lg > row_max + col_max) {
         // three levels: rows of the longest row kernel (fewest samples in
         // the two column levels), the column lengths and kernels varied
         for (int l1 = 4; l1 <= col_max; ++l1) {
@@ -1011,7 +1022,8 @@ rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double
             if (lb < 4 || lb > col_max) continue;
             for (int ce : {16, 8})
                 for (int me : {16, 8})
-                    if (col_e_ok(l1, ce) && col_e_ok(lb, me)) cands.push_back(rsw_tuning{3, l1, lb, 16, ce, me});
+                    if (col_e_ok(l1, ce, c128) && col_e_ok(lb, me, c128))
+                        cands.push_back(rsw_tuning{3, l1, lb, 16, ce, me});
         }
     }
     cudaStream_t s = (cudaStream_t)stream;

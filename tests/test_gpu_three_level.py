@@ -21,6 +21,7 @@ if not torch.cuda.is_available():
 
 import rave_sim_b200 as rsw  # noqa: E402
 from rave_sim_b200 import workloads  # noqa: E402
+from rave_sim_b200.autotune import plan_tuning  # noqa: E402
 
 DEV = "cuda"
 TOL_FFT = {"c16": 1e-12, "c8": 2e-6}
@@ -117,12 +118,15 @@ def test_three_level_matches_two_level_talbot_lau(split3):
     assert rel_l2(three, two) < 1e-12
 
 
-@pytest.mark.parametrize("dt,logn", [("c16", 25), ("c8", 27)])
-def test_plans_above_the_two_level_limit(dt, logn):
+# 2^25 c16: two levels with columns of 2^12 (two-column tiles); 2^26 c16 and
+# 2^27 c8: three levels
+@pytest.mark.parametrize("dt,logn,levels", [("c16", 25, 2), ("c16", 26, 3), ("c8", 27, 3)])
+def test_plans_above_the_two_level_limit(dt, logn, levels):
     n = 1 << logn
     p = rsw.Plan(n, dt)
     info = p.info()
     assert info["log_rows"] + info["log_cols"] == logn
+    assert plan_tuning(p)["levels"] == levels
     x = to_dev(cplx(n, 11, dt))
     X = p.fft(x, torch.empty_like(x))
     ref = torch.fft.fft(x.to(torch.complex128))
