@@ -75,6 +75,9 @@ def parse():
                     help="use the built-in schedule instead of timing the candidates first")
     ap.add_argument("--no-gpu-baseline", action="store_true",
                     help="skip the reference's cuFFT fast-wave path on the same workload")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="run the sources of a field length one after the other instead of in lockstep "
+                         "(one launch per pass for all of them)")
     a = ap.parse_args()
     if a.dtype is None:
         a.dtype = "c16" if a.workload == "talbot_lau" else "c8"
@@ -344,6 +347,7 @@ def main():
     for g in groups:
         g["stream"] = torch.cuda.Stream() if len(groups) > 1 else main_stream
     sim0 = groups[0]["sim"]
+    batch = not args.no_batch
     acc = torch.zeros((sim0.nr_phase_steps, sim0.n_pix), dtype=torch.float64, device=dev)
     accs = [torch.zeros_like(acc) for _ in groups]
 
@@ -355,8 +359,12 @@ def main():
                 sim.reset()
                 src = g["case"]["source"] if fields is None else {"type": "vector", "z": g["case"]["source"]["z"]}
                 f = None if fields is None else fields[i]
-                for e, w in zip(g["energies"], g["weights"]):
-                    sim.run_source(energy=e, db_table=g["db"](e), source=src, weight=w, field=f)
+                if batch:
+                    sim.run_sources([{"energy": e, "db_table": g["db"](e), "weight": w}
+                                     for e, w in zip(g["energies"], g["weights"])], source=src, field=f)
+                else:
+                    for e, w in zip(g["energies"], g["weights"]):
+                        sim.run_source(energy=e, db_table=g["db"](e), source=src, weight=w, field=f)
                 sim.detected_device(accs[i])
         for g in groups:
             main_stream.wait_stream(g["stream"])
@@ -442,14 +450,21 @@ def main():
         e2e_ms = max_over_ranks(ev2.elapsed_time(ev3)) / e2e_steps
         e2e_value = total_samples / (e2e_ms * 1e-3)
 
-    # ---- per-kernel device time (CUDA events on the launch stream), one
-    # energy of the largest field
+    # ---- per-kernel device time (CUDA events on the launch stream): the
+    # largest field's sources as the timed region runs them (a lockstep batch
+    # of all of them, or one energy)
     gd = max(groups, key=lambda g: g["n"])
     n = gd["n"]
     sim = gd["sim"]
     sim.set_timing(True)
-    e = gd["energies"][0]
-    sim.run_source(energy=e, db_table=gd["db"](e), source=gd["case"]["source"], weight=0.0)
+    if batch:
+        sim.run_sources([{"energy": e, "db_table": gd["db"](e), "weight": 0.0} for e in gd["energies"]],
+                        source=gd["case"]["source"])
+        per_launch = len(gd["energies"])  # fields per pass launch
+    else:
+        e = gd["energies"][0]
+        sim.run_source(energy=e, db_table=gd["db"](e), source=gd["case"]["source"], weight=0.0)
+        per_launch = 1
     kinds = {}
     for k, name in ((0, "row_pass"), (1, "col_pass"), (2, "detect"), (3, "mid_pass")):
         t, cnt = sim.timing(k)
@@ -459,7 +474,7 @@ def main():
     passes = [k for k in ("row_pass", "col_pass", "mid_pass") if k in kinds and kinds[k]["launches"]]
     dom = max(passes, key=lambda k: kinds[k]["ms_total"])
     avg_ms = kinds[dom]["ms_avg"]
-    algo_bytes = 2.0 * n * s_bytes  # read + write of the field per pass launch
+    algo_bytes = 2.0 * n * s_bytes * per_launch  # read + write of the fields per pass launch
     peak, peak_kind = measured_peak_hbm()
     achieved = algo_bytes / (avg_ms * 1e-3) / 1e9
     for k in passes:
@@ -470,6 +485,10 @@ def main():
                 "algorithmic_bytes_per_launch": algo_bytes,
                 "kernels": kinds}
     roofline["traffic"], roofline["traffic_source"] = ncu_traffic(dom, args.dtype, int(round(math.log2(n))))
+    if roofline["traffic"] is not None and per_launch > 1:
+        roofline["traffic"] *= per_launch
+        roofline["traffic_source"] += f", times the {per_launch} fields of a batched launch"
+    roofline["fields_per_launch"] = per_launch
 
     # ---- mixed precision against the complex128 run of the same step
     precision = None
@@ -478,8 +497,8 @@ def main():
         for g, a in zip(groups, accs):
             s16 = rsw.Simulation(g["case"], grids=g["grids"], dtype="c16")
             s16.reset()
-            for e, w in zip(g["energies"], g["weights"]):
-                s16.run_source(energy=e, db_table=g["db"](e), source=g["case"]["source"], weight=w)
+            s16.run_sources([{"energy": e, "db_table": g["db"](e), "weight": w}
+                             for e, w in zip(g["energies"], g["weights"])], source=g["case"]["source"])
             ref += s16.detected_device()
             s16.close()
         run_step()
@@ -512,6 +531,8 @@ def main():
                "l2_policy": "inputs larger than L2" if n * s_bytes > (126 << 20) else
                             "field smaller than L2 (no flush)",
                "parallelism": f"dp{ws} (energies sharded, detector all-reduce)",
+               "sources": "lockstep batch per field length (one launch per pass for all its energies)"
+                          if batch else "one source after the other",
                "schedule": {"autotuned": tuning} if tuning else "built-in"}
         if args.workload == "talbot_lau":
             cfg.update({"n": n, "energies_per_rank": len(gd["energies"]), "field_bytes": n * s_bytes,

@@ -302,6 +302,23 @@ rsw_status rsw_sim_shape(rsw_sim sim, int64_t *nr_phase_steps, int64_t *n_pix,
  * accumulator. Asynchronous on `stream`. */
 rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run *run,
                        void *stream);
+/* Run `count` sources (runs[0 .. count-1]: energies, deltabeta, weights) of
+ * the same source geometry in lockstep. Replaces the reference's one run per
+ * source (big-wave/wavesim.py:84-298 called once per energy by
+ * big-wave/multisim.py:50-150; fast-wave's one invocation per source index,
+ * fast-wave/Readme.md:22-26): every split step of all sources is one launch
+ * per pass over count * N samples, each source an instance with its own
+ * wavelength-dependent factors, transfer function and chirp table, and the
+ * detector values are added in source order, as count rsw_sim_run calls would
+ * add them. The sim keeps batch buffers of count * N samples (two with phase
+ * stepping), sized for the largest batch run so far. Lockstep needs a plan
+ * of two or three levels, the Fresnel propagator, no history, no keypoints,
+ * at least one element and a detector of at least one pixel; otherwise the
+ * sources run one after the other through rsw_sim_run. A batch keeps no
+ * final field (rsw_sim_final_field). count <= RSW_BATCH_MAX. */
+#define RSW_BATCH_MAX 4096
+rsw_status rsw_sim_run_batch(rsw_sim sim, const rsw_source *src, const rsw_source_run *runs,
+                             int64_t count, void *stream);
 /* Zero the accumulator. */
 rsw_status rsw_sim_reset(rsw_sim sim, void *stream);
 /* Copy the accumulator (nr_phase_steps * n_pix doubles) to host memory;

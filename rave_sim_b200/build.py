@@ -28,9 +28,10 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
 ]
 
-SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_col_det.cu", "rsw_kernels.cu", "rsw_noalloc.cu",
-           "rsw_host.cpp"]
-HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh", "rsw_stages.h", "rsw_col_dispatch.h"]
+SOURCES = ["rsw_row_f64.cu", "rsw_row_f32.cu", "rsw_col.cu", "rsw_col_det.cu", "rsw_row_f64_batch.cu",
+           "rsw_row_f32_batch.cu", "rsw_col_batch.cu", "rsw_kernels.cu", "rsw_noalloc.cu", "rsw_host.cpp"]
+HEADERS = ["rsw_block_fft.cuh", "rsw_internal.h", "rsw_passes.cuh", "rsw_stages.h", "rsw_col_dispatch.h",
+           "rsw_row_dispatch.h"]
 
 
 def nvcc() -> str:

@@ -2,7 +2,10 @@
 #include "rsw_col_dispatch.h"
 
 namespace rsw {
+cudaError_t launch_col_pass_batch(const PassArgs &a, bool dbl, int e, cudaStream_t s);
+// per-instance transmission factors take the batched kernels (rsw_col_batch.cu)
 cudaError_t launch_col_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) {
+    if (a.btr) return launch_col_pass_batch(a, dbl, e, s);
     return col_dispatch<false>(a, dbl, e, s);
 }
 

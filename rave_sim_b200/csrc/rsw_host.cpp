@@ -662,8 +662,12 @@ static PassArgs base_args(const rsw_plan_s *p) {
     a.rb_nb = digit_bits(p->mid_e);
     a.pr.fac = 1.0 / double(p->n);
     a.tr.kind = TR_NONE;
+    a.det.n_inst = 1;
     return a;
 }
+// detector sums of one instance of a batched detection pass: n_pix doubles
+// rounded up to a 256-byte multiple
+static int64_t batch_sum_stride(int64_t n_pix) { return (n_pix + 31) / 32 * 32; }
 // The same arguments for the row kernel: rows of Nr samples; in three-level
 // plans its twiddles are W_{N2}^(nr kb), unscaled.
 static PassArgs row_level(const rsw_plan_s *p, PassArgs a) {
@@ -810,6 +814,7 @@ static rsw_status launch_split_step(const rsw_plan_s *P, PassArgs a, bool mid_in
         CHECK(run_col(P, a, st, tl));
         a.in = out;
         a.tr.kind = TR_NONE;
+        a.btr = nullptr;
         if (P->three()) CHECK(run_mid(P, a, true, st, tl));
         a.pr = keep;
         PassArgs r = row_level(P, a);
@@ -1617,6 +1622,13 @@ struct SimElement {
     }
 };
 
+// transfer-function tables of one (dz, cutoff) for the instances of a batch
+struct BatchPropTables {
+    DevBuf entries, h3;
+    std::vector<BatchProp> host;
+    bool any_cut = false;
+};
+
 struct rsw_sim_s {
     rsw_plan_s *plan = nullptr;
     rsw_sim_desc d{};
@@ -1644,6 +1656,14 @@ struct rsw_sim_s {
     // keypoints (big-wave/wavesim.py:35-55): caller buffers for the field
     // before / after each element of the first pass, NULL entries skipped
     std::vector<void *> keypoints;
+    // lockstep batches (rsw_sim_run_batch), sized for the largest batch so far:
+    // field buffers of nb * N samples, per-instance transmission entries
+    // [element][grating, substrate][instance], sample material tables
+    // [instance][element][128], transfer-function tables per (dz, cutoff),
+    // detector sums [instance][sum_stride] then the CTA counter, weights
+    int64_t batch_cap = 0;
+    DevBuf bbuf[2], btab, bmat_db, bmat_fac, bsum, bweight;
+    std::vector<std::unique_ptr<BatchPropTables>> bprop;
     ~rsw_sim_s() { rsw_plan_destroy(plan); }
 };
 
@@ -1678,6 +1698,16 @@ struct Runner {
     // per-run material factors: per element [fa? ...]
     std::vector<std::vector<cplx>> db;  // deltabeta per element (gratings: a,b,sub; samples: materials 1..)
     std::vector<double> chirp_dz;       // dz of each built chirp table of this run (slot = index)
+    // Lockstep batches (rsw_sim_run_batch): nb instances of the same field
+    // length in consecutive N-sample slices of the batch buffers; instance 0's
+    // values stand in the common arguments, the wavelength-dependent ones of
+    // every instance come from device tables
+    int nb = 1;
+    DevBuf *fbuf = nullptr;                // field buffers: the sim's own, or its batch buffers
+    std::vector<double> wls;               // wavelength per instance
+    std::vector<std::vector<double>> cuts; // cutoff frequency per instance and cutoff index
+    const BatchTrans *btr = nullptr;       // entries of the element being applied
+    std::vector<std::pair<double, int>> prop_keys;  // (dz, cutoff index) of each transfer-function table
 
     // chirp table for a distance dz at this run's wavelength (built on first use)
     rsw_status chirp_for(PropArgs &pr, double dz) {
@@ -1706,19 +1736,75 @@ struct Runner {
         return cur == readonly ? 1 - cur : cur;
     }
     // field buffers 0 and 1 hold the state; 2 is the history buffer
-    void *bp(int i) const { return i == 2 ? S->hbuf.p : S->buf[i].p; }
+    void *bp(int i) const { return i == 2 ? S->hbuf.p : fbuf[i].p; }
 
-    rsw_status split_step(const TransArgs &tr, double dz, double cutoff) {
-        return step_to(tr, dz, cutoff, target(), true);
+    // batch: the instances' transmission entries of element ei (sub 0: the
+    // grating or sample, 1: the substrate)
+    const BatchTrans *btab_at(int ei, int sub) const {
+        return static_cast<const BatchTrans *>(S->btab.p) + (size_t(ei) * 2 + size_t(sub)) * size_t(nb);
     }
+    // batch: the instances' transfer functions of a split step over dz with
+    // cutoff ci (built on first use in a run: the scalars of make_prop and
+    // chirp_constant per instance and one chirp table each); pr keeps
+    // instance 0's common values and covers every instance's cutoff
+    rsw_status batch_prop(PropArgs &pr, double dz, int ci, const BatchProp **out) {
+        size_t slot = 0;
+        while (slot < prop_keys.size() && !(prop_keys[slot].first == dz && prop_keys[slot].second == ci)) ++slot;
+        const bool chirp = pr.has_h && !pr.exact;
+        const size_t nr = size_t(1) << P->log_nr;
+        if (slot == prop_keys.size()) {
+            prop_keys.emplace_back(dz, ci);
+            if (S->bprop.size() <= slot) S->bprop.emplace_back(new BatchPropTables());
+            BatchPropTables &t = *S->bprop[slot];
+            CHECK(t.entries.alloc(size_t(nb) * sizeof(BatchProp)));
+            if (chirp) CHECK(t.h3.alloc(size_t(nb) * nr * 16));
+            t.host.assign(size_t(nb), BatchProp{});
+            t.any_cut = false;
+            for (int b = 0; b < nb; ++b) {
+                PropArgs q = make_prop(P->n, S->d.dx, wls[size_t(b)], dz, cuts[size_t(b)][size_t(ci)], dz != 0.0);
+                BatchProp &e = t.host[size_t(b)];
+                e.A = q.A;
+                if (q.has_cut) {
+                    e.cut_lo = q.cut_lo;
+                    e.cut_hi = q.cut_hi;
+                    t.any_cut = true;
+                }
+                if (chirp) {
+                    void *h3 = static_cast<char *>(t.h3.p) + size_t(b) * nr * 16;
+                    CHECK(prepare_chirp(P, q, h3, st));
+                    e.g_hi = q.g_hi;
+                    e.g_lo = q.g_lo;
+                    e.h3 = h3;
+                }
+            }
+            // pageable source: staged before the call returns
+            CU(cudaMemcpyAsync(t.entries.p, t.host.data(), t.host.size() * sizeof(BatchProp), cudaMemcpyHostToDevice,
+                               st));
+        }
+        const BatchPropTables &t = *S->bprop[slot];
+        pr.has_cut = t.any_cut ? 1 : 0;
+        if (chirp) pr.chirp = 1;
+        *out = static_cast<const BatchProp *>(t.entries.p);
+        return RSW_OK;
+    }
+
+    rsw_status split_step(const TransArgs &tr, double dz, int ci) { return step_to(tr, dz, ci, target(), true); }
 
     // One split step from the current state into buffer dst; commit = false
     // leaves the state untouched (history points reached from a gap start).
-    rsw_status step_to(const TransArgs &tr, double dz, double cutoff, int dst, bool commit) {
+    // ci: the cutoff's index (the element the step belongs to, 0 before the
+    // first one).
+    rsw_status step_to(const TransArgs &tr, double dz, int ci, int dst, bool commit) {
         PassArgs a = base_args(P);
         a.tr = tr;
-        a.pr = make_prop(P->n, S->d.dx, wl, dz, cutoff, dz != 0.0, P->prop_mode == RSW_PROP_EXACT);
-        CHECK(chirp_for(a.pr, dz));
+        a.pr = make_prop(P->n, S->d.dx, wl, dz, cut[size_t(ci)], dz != 0.0, P->prop_mode == RSW_PROP_EXACT);
+        if (nb > 1) {
+            a.n = P->n * nb;
+            CHECK(batch_prop(a.pr, dz, ci, &a.bpr));
+            a.btr = tr.kind != TR_NONE ? btr : nullptr;
+        } else {
+            CHECK(chirp_for(a.pr, dz));
+        }
         a.in = ones ? nullptr : bp(cur);
         a.out = bp(dst);
         bool now_mid = false;
@@ -1740,7 +1826,7 @@ struct Runner {
             ones = false;
             mid = now_mid;
         }
-        ++S->split_steps;
+        S->split_steps += nb;
         return RSW_OK;
     }
 
@@ -1811,12 +1897,12 @@ struct Runner {
     // propagate_with_history (big-wave/history.py:67-135): every history point
     // is reached from the state at the start of the gap; the last one is the
     // gap's own propagation
-    rsw_status gap(double dz, double cutoff, double z_from) {
+    rsw_status gap(double dz, int ci, double z_from) {
         if (dz == 0.0) return RSW_OK;
-        if (!hist_on) return split_step(TransArgs{}, dz, cutoff);
+        if (!hist_on) return split_step(TransArgs{}, dz, ci);
         const std::vector<double> zs = history_zs(dz, S->hist_dz);
         for (size_t i = 1; i + 1 < zs.size(); ++i) {
-            CHECK(step_to(TransArgs{}, zs[i] - zs[0], cutoff, 2, false));
+            CHECK(step_to(TransArgs{}, zs[i] - zs[0], ci, 2, false));
             if (P->log_n1 > 0) {  // "mid" -> natural, in place
                 PassArgs a = base_args(P);
                 a.in = bp(2);
@@ -1826,7 +1912,7 @@ struct Runner {
             }
             CHECK(hist_detect(bp(2), zs[i] + z_from));
         }
-        CHECK(split_step(TransArgs{}, zs.back() - zs[0], cutoff));
+        CHECK(split_step(TransArgs{}, zs.back() - zs[0], ci));
         return hist_push(zs.back() + z_from);
     }
 
@@ -1884,8 +1970,9 @@ struct Runner {
         }
         const int dst = target();
         PassArgs a = base_args(P);
-        a.in = S->buf[cur].p;
-        a.out = S->buf[dst].p;
+        a.n = P->n * nb;
+        a.in = bp(cur);
+        a.out = bp(dst);
         a.flags = col_inv(P) | (keep ? 0 : PF_NOSTORE);
         DetectArgs &d = a.det;
         d.bounds = (const int64_t *)S->bounds.p;
@@ -1902,6 +1989,13 @@ struct Runner {
         d.count = (unsigned *)((double *)S->dsum.p + np);
         d.acc = (double *)S->acc.p + phase * np;
         d.comp = (double *)S->comp.p + phase * np;
+        if (nb > 1) {
+            d.sum_stride = batch_sum_stride(np);
+            d.sum = (double *)S->bsum.p;
+            d.count = (unsigned *)(d.sum + nb * d.sum_stride);
+            d.bweight = (const double *)S->bweight.p;
+            d.n_inst = nb;
+        }
         TimingLog::Rec r{};
         if (S->tl.enabled) S->tl.begin(2, st, r);
         cudaError_t e = launch_col_detect(a, P->dbl(), P->col_e, st);
@@ -1927,7 +2021,7 @@ struct Runner {
         return RSW_OK;
     }
 
-    rsw_status apply(int ei, int64_t step, double cutoff) {
+    rsw_status apply(int ei, int64_t step, int ci) {
         SimElement &el = S->els[ei];
         const rsw_element &e = el.d;
         const std::vector<cplx> &m = db[ei];
@@ -1957,7 +2051,8 @@ struct Runner {
                     tr.chunk_xstart = (const double *)el.chunk_xs[step]->p;
                     tr.chunk_step = (const double *)el.chunk_st[step]->p;
                 }
-                CHECK(split_step(tr, z_step, cutoff));
+                if (nb > 1) btr = btab_at(ei, 0);
+                CHECK(split_step(tr, z_step, ci));
                 if (hist_on) CHECK(hist_push(e.z_start + double(i + 1) * z_step));
             }
             if (e.substrate_thickness > 0) {
@@ -1965,7 +2060,8 @@ struct Runner {
                 TransArgs tr{};
                 tr.kind = TR_SCALAR;
                 tr.fa = make_double2(fs.real(), fs.imag());
-                CHECK(split_step(tr, e.substrate_thickness, cutoff));
+                if (nb > 1) btr = btab_at(ei, 1);
+                CHECK(split_step(tr, e.substrate_thickness, ci));
             }
             return RSW_OK;
         }
@@ -1987,7 +2083,8 @@ struct Runner {
         for (int64_t r = 0; r < e.grid_z; ++r) {
             if (hist_on) CHECK(hist_push(e.z_start + double(r) * psz));
             tr.row_grid = (const int8_t *)el.grid_dev.p + r * e.grid_x;
-            CHECK(split_step(tr, psz, cutoff));
+            if (nb > 1) btr = btab_at(ei, 0);
+            CHECK(split_step(tr, psz, ci));
         }
         return RSW_OK;
     }
@@ -2199,33 +2296,28 @@ rsw_status rsw_sim_history(rsw_sim S, double *h_out, double *h_z, int64_t *n_ent
     return RSW_OK;
 }
 
-rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
-    if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
-    if (!(run->energy_ev > 0) && !(run->wavelength_m > 0))
-        return fail(RSW_ERR_INVALID, "energy or wavelength must be positive");
-    ++g_api_calls;
-    Runner R;
-    R.S = S;
-    R.P = S->plan;
-    R.st = (cudaStream_t)stream;
-    R.wl = run->wavelength_m > 0 ? run->wavelength_m : wavelength(run->energy_ev);
-    for (double a : S->cutoff_angles) R.cut.push_back(std::sin(a) / R.wl);
-    // deltabeta per element
+}  // extern "C"
+
+namespace {
+
+// The deltabeta values of one run per element (gratings: a, b, substrate;
+// samples: materials 1..n), and the host images of its sample material tables
+// (deltabeta and exp(i y db) at [element * 128 + material], [0] = vacuum).
+static rsw_status load_deltabeta(const rsw_sim_s &S, const rsw_source_run *run, double wl,
+                                 std::vector<std::vector<cplx>> &db, double *dbh, double *fch) {
     int64_t k = 0;
-    std::vector<double> dbh(size_t(std::max<int64_t>(S->d.n_elements, 1)) * 128 * 2, 0.0);
-    std::vector<double> fch(dbh.size(), 0.0);
-    R.db.resize(S->els.size());
-    for (size_t i = 0; i < S->els.size(); ++i) {
-        const rsw_element &e = S->els[i].d;
+    db.assign(S.els.size(), {});
+    for (size_t i = 0; i < S.els.size(); ++i) {
+        const rsw_element &e = S.els[i].d;
         const int cnt = e.type == RSW_EL_SAMPLE ? e.n_materials : 3;
         if (k + cnt > run->n_deltabeta || (cnt > 0 && !run->deltabeta))
             return fail(RSW_ERR_INVALID, "deltabeta table too short (%lld values)", (long long)run->n_deltabeta);
-        for (int m = 0; m < cnt; ++m, ++k) R.db[i].push_back(cplx(run->deltabeta[2 * k], run->deltabeta[2 * k + 1]));
+        for (int m = 0; m < cnt; ++m, ++k) db[i].push_back(cplx(run->deltabeta[2 * k], run->deltabeta[2 * k + 1]));
         if (e.type == RSW_EL_SAMPLE) {
             const double psz = e.pixel_size_z;
             for (int m = 0; m < cnt; ++m) {
-                const cplx d = R.db[i][m];
-                const cplx f = material_factor(d.real(), d.imag(), psz, R.wl);
+                const cplx d = db[i][m];
+                const cplx f = material_factor(d.real(), d.imag(), psz, wl);
                 dbh[(i * 128 + m + 1) * 2] = d.real();
                 dbh[(i * 128 + m + 1) * 2 + 1] = d.imag();
                 fch[(i * 128 + m + 1) * 2] = f.real();
@@ -2234,14 +2326,22 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
             fch[(i * 128) * 2] = 1.0;
         }
     }
-    CU(cudaMemcpyAsync(S->mat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
-    CU(cudaMemcpyAsync(S->mat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
+    return RSW_OK;
+}
 
-    rsw_sim_s &s = *S;
+static double run_wavelength(const rsw_source_run *run) {
+    return run->wavelength_m > 0 ? run->wavelength_m : wavelength(run->energy_ev);
+}
+
+// The per-source schedule of big-wave/wavesim.py:84-298 on R's instances:
+// source, elements (phase-step snapshot before the first stepped element),
+// detector, then the remaining phase steps from the snapshot.
+static rsw_status run_schedule(Runner &R, const rsw_source *src, double weight) {
+    rsw_sim_s &s = *R.S;
     const double z_tol = 1e-8;
     const int nel = int(s.els.size());
     // ---- source (big-wave/source.py:46-101)
-    double cutoff = R.cut[0];
+    int ci = 0;  // cutoff index: R.cut[ci]
     double z = nel > 0 ? s.els[0].d.z_start : s.d.z_detector;
     R.cur = 0;
     R.readonly = -1;
@@ -2250,24 +2350,30 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     s.hist_z.clear();
     R.hist_on = s.hist_dz > 0;
     if (R.hist_on) CHECK(s.hbuf.alloc(size_t(s.d.n) * R.P->elem()));
+    const size_t fbytes = size_t(s.d.n) * R.P->elem();
     if (src->type == RSW_SRC_POINT) {
-        // grid_density_check (big-wave/propagation.py:31-45)
+        // grid_density_check (big-wave/propagation.py:31-45), per instance
         const double dzs = z - src->z;
         auto dist_x = [&](double idx) {
             const double a = (double(s.d.n) / 2.0 - idx) * s.d.dx + std::fabs(src->x);
             return std::sqrt(a * a + dzs * dzs);
         };
-        if (!(std::fabs(dist_x(0.0) - dist_x(1.0)) <= R.wl / 2.0))
-            return fail(RSW_ERR_INVALID, "Nyquist not satisfied, dx too large for the point source at dz = %g", dzs);
-        CHECK(rsw_point_source(R.P, s.buf[0].p, s.d.dx, R.wl, z - src->z, src->x, stream));
-        CHECK(R.split_step(TransArgs{}, 0.0, cutoff));
+        for (int b = 0; b < R.nb; ++b) {
+            const double wl = R.wls[size_t(b)];
+            if (!(std::fabs(dist_x(0.0) - dist_x(1.0)) <= wl / 2.0))
+                return fail(RSW_ERR_INVALID, "Nyquist not satisfied, dx too large for the point source at dz = %g",
+                            dzs);
+            CHECK(rsw_point_source(R.P, static_cast<char *>(R.bp(0)) + size_t(b) * fbytes, s.d.dx, wl, z - src->z,
+                                   src->x, (void *)R.st));
+        }
+        CHECK(R.split_step(TransArgs{}, 0.0, ci));
         if (R.hist_on) {
             // generate_analytic_history (big-wave/history.py:43-64) at
             // np.arange(0, z, hdz)[1:]
             const double psx = s.d.pixel_size_x, psy = s.d.pixel_size_y;
             const double nd = py_floordiv(s.d.detector_size, psx);
             const int64_t npx = int64_t(nd);
-            const double gradient = cutoff * R.wl;
+            const double gradient = R.cut[0] * R.wl;
             const int64_t len = std::max<int64_t>(int64_t(std::ceil(z / s.hist_dz)), 0);
             for (int64_t k = 1; k < len; ++k) {
                 const double zh = double(k) * s.hist_dz;
@@ -2285,15 +2391,17 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
         if (src->type == RSW_SRC_PLANE) {
             R.ones = true;
             R.cur = -1;
-        } else if (src->d_field) {
-            CU(cudaMemcpyAsync(s.buf[0].p, src->d_field, size_t(s.d.n) * R.P->elem(), cudaMemcpyDeviceToDevice, R.st));
-        } else if (src->h_field) {
-            CU(cudaMemcpyAsync(s.buf[0].p, src->h_field, size_t(s.d.n) * R.P->elem(), cudaMemcpyHostToDevice, R.st));
+        } else if (src->d_field || src->h_field) {
+            // the same input field for every instance
+            const cudaMemcpyKind kind = src->d_field ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+            const void *from = src->d_field ? src->d_field : src->h_field;
+            for (int b = 0; b < R.nb; ++b)
+                CU(cudaMemcpyAsync(static_cast<char *>(R.bp(0)) + size_t(b) * fbytes, from, fbytes, kind, R.st));
         } else {
             return fail(RSW_ERR_INVALID, "vector source without a field");
         }
         const double dz = z - src->z;
-        if (dz != 0.0) CHECK(R.gap(dz, cutoff, src->z));
+        if (dz != 0.0) CHECK(R.gap(dz, ci, src->z));
     } else {
         return fail(RSW_ERR_INVALID, "unknown source type %d", src->type);
     }
@@ -2306,21 +2414,22 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     } snap{0, -1, false, false};
     for (int i = 0; i < nel; ++i) {
         const rsw_element &e = s.els[i].d;
-        if (z < e.z_start) CHECK(R.gap(e.z_start - z, cutoff, z));
+        if (z < e.z_start) CHECK(R.gap(e.z_start - z, ci, z));
         z = e.z_start;
         if (i == s.snap_el) {
             snap = Snap{z, R.cur, R.mid, R.ones};
             R.readonly = R.cur;
         }
-        cutoff = R.cut[i + 1];
+        ci = i + 1;
         const bool kp = s.keypoints.size() == size_t(2 * nel);
         if (kp) CHECK(R.keypoint(s.keypoints[size_t(2 * i)]));
-        CHECK(R.apply(i, 0, cutoff));
+        CHECK(R.apply(i, 0, ci));
         if (kp) CHECK(R.keypoint(s.keypoints[size_t(2 * i + 1)]));
         z = e.z_start + s.els[i].total_thickness();
     }
-    if (z < s.d.z_detector - z_tol) CHECK(R.gap(s.d.z_detector - z, cutoff, z));
-    CHECK(R.finish_phase(0, run->weight, s.nr_phase_steps == 1));
+    if (z < s.d.z_detector - z_tol) CHECK(R.gap(s.d.z_detector - z, ci, z));
+    const bool batched = R.nb > 1;  // batches keep no final field
+    CHECK(R.finish_phase(0, weight, s.nr_phase_steps == 1 && !batched));
     R.hist_on = false;  // phase steps from the snapshot record no history (big-wave/wavesim.py:234-237)
 
     // ---- remaining phase steps from the snapshot (big-wave/wavesim.py:238-296)
@@ -2329,20 +2438,138 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
         R.mid = snap.mid;
         R.ones = snap.ones;
         z = snap.z;
-        cutoff = R.cut[s.snap_el];
+        ci = s.snap_el;
         for (int i = s.snap_el; i < nel; ++i) {
             const rsw_element &e = s.els[i].d;
-            if (z < e.z_start) CHECK(R.split_step(TransArgs{}, e.z_start - z, cutoff));
+            if (z < e.z_start) CHECK(R.split_step(TransArgs{}, e.z_start - z, ci));
             z = e.z_start;
-            cutoff = R.cut[i + 1];
-            CHECK(R.apply(i, e.n_x_positions > 1 ? step : 0, cutoff));
+            ci = i + 1;
+            CHECK(R.apply(i, e.n_x_positions > 1 ? step : 0, ci));
             z = e.z_start + s.els[i].total_thickness();
         }
-        if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, cutoff));
-        CHECK(R.finish_phase(step, run->weight, step == s.nr_phase_steps - 1));
+        if (z < s.d.z_detector - z_tol) CHECK(R.split_step(TransArgs{}, s.d.z_detector - z, ci));
+        CHECK(R.finish_phase(step, weight, step == s.nr_phase_steps - 1 && !batched));
     }
-    s.last_field = R.cur;
+    s.last_field = batched ? -1 : R.cur;
     return RSW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
+    if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (!(run->energy_ev > 0) && !(run->wavelength_m > 0))
+        return fail(RSW_ERR_INVALID, "energy or wavelength must be positive");
+    ++g_api_calls;
+    Runner R;
+    R.S = S;
+    R.P = S->plan;
+    R.st = (cudaStream_t)stream;
+    R.fbuf = S->buf;
+    R.wl = run_wavelength(run);
+    R.wls.assign(1, R.wl);
+    for (double a : S->cutoff_angles) R.cut.push_back(std::sin(a) / R.wl);
+    std::vector<double> dbh(size_t(std::max<int64_t>(S->d.n_elements, 1)) * 128 * 2, 0.0);
+    std::vector<double> fch(dbh.size(), 0.0);
+    CHECK(load_deltabeta(*S, run, R.wl, R.db, dbh.data(), fch.data()));
+    CU(cudaMemcpyAsync(S->mat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
+    CU(cudaMemcpyAsync(S->mat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
+    return run_schedule(R, src, run->weight);
+}
+
+rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
+                             void *stream) {
+    if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (count < 0 || count > RSW_BATCH_MAX)
+        return fail(RSW_ERR_INVALID, "batch of %lld sources (at most %d)", (long long)count, RSW_BATCH_MAX);
+    for (int64_t b = 0; b < count; ++b)
+        if (!(runs[b].energy_ev > 0) && !(runs[b].wavelength_m > 0))
+            return fail(RSW_ERR_INVALID, "source %lld: energy or wavelength must be positive", (long long)b);
+    rsw_plan_s *P = S->plan;
+    // lockstep needs the two- or three-level passes with the chirp form of the
+    // Fresnel kernel and the fused detection; everything else runs the
+    // sources one after the other, with the same results
+    const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
+                          S->hist_dz == 0.0 && S->keypoints.empty() && !S->els.empty() && S->geom.n_pix > 0;
+    if (!lockstep) {
+        for (int64_t b = 0; b < count; ++b) CHECK(rsw_sim_run(S, src, runs + b, stream));
+        return RSW_OK;
+    }
+    ++g_api_calls;
+    const int nb = int(count);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nel = S->els.size();
+    const int64_t np = S->geom.n_pix;
+    const int64_t stride = batch_sum_stride(np);
+    if (S->batch_cap < nb) {
+        // sums and counter start at zero and are left at zero by every pass
+        const size_t fb = size_t(S->d.n) * P->elem() * size_t(nb);
+        CHECK(S->bbuf[0].alloc(fb));
+        if (S->nr_phase_steps > 1) CHECK(S->bbuf[1].alloc(fb));
+        CHECK(S->btab.alloc(nel * 2 * size_t(nb) * sizeof(BatchTrans)));
+        CHECK(S->bmat_db.alloc(size_t(nb) * nel * 128 * sizeof(double2)));
+        CHECK(S->bmat_fac.alloc(size_t(nb) * nel * 128 * sizeof(double2)));
+        const size_t sum_bytes = size_t(nb * stride) * sizeof(double) + 16;
+        CHECK(S->bsum.alloc(sum_bytes));
+        CU(cudaMemsetAsync(S->bsum.p, 0, sum_bytes, st));
+        CHECK(S->bweight.alloc(size_t(nb) * sizeof(double)));
+        S->batch_cap = nb;
+    }
+    Runner R;
+    R.S = S;
+    R.P = P;
+    R.st = st;
+    R.nb = nb;
+    R.fbuf = S->bbuf;
+    R.cuts.resize(size_t(nb));
+    std::vector<double> dbh(size_t(nb) * nel * 128 * 2, 0.0), fch(dbh.size(), 0.0);
+    std::vector<BatchTrans> tab(nel * 2 * size_t(nb));
+    std::vector<double> weights(static_cast<size_t>(nb));
+    const double2 *mdb = static_cast<const double2 *>(S->bmat_db.p);
+    const double2 *mfc = static_cast<const double2 *>(S->bmat_fac.p);
+    for (int b = 0; b < nb; ++b) {
+        const rsw_source_run *run = runs + b;
+        const double wl = run_wavelength(run);
+        R.wls.push_back(wl);
+        for (double a : S->cutoff_angles) R.cuts[size_t(b)].push_back(std::sin(a) / wl);
+        std::vector<std::vector<cplx>> db;
+        const size_t off = size_t(b) * nel * 128 * 2;
+        CHECK(load_deltabeta(*S, run, wl, db, dbh.data() + off, fch.data() + off));
+        // the wavelength-dependent transmission values of each element
+        // (Runner::apply computes the same for one source)
+        for (size_t i = 0; i < nel; ++i) {
+            const rsw_element &e = S->els[i].d;
+            BatchTrans &t0 = tab[(i * 2) * size_t(nb) + size_t(b)];
+            BatchTrans &t1 = tab[(i * 2 + 1) * size_t(nb) + size_t(b)];
+            if (e.type == RSW_EL_SAMPLE) {
+                t0.mat_db = mdb + (size_t(b) * nel + i) * 128;
+                t0.mat_factor = mfc + (size_t(b) * nel + i) * 128;
+                t0.sample_y = (2.0 * M_PI * e.pixel_size_z) / wl;
+            } else {
+                const double z_step = e.thickness / double(e.nr_steps);
+                const cplx fa = material_factor(db[i][0].real(), db[i][0].imag(), z_step, wl);
+                const cplx fb = material_factor(db[i][1].real(), db[i][1].imag(), z_step, wl);
+                t0.fa = make_double2(fa.real(), fa.imag());
+                t0.fb = make_double2(fb.real(), fb.imag());
+                const cplx fs = material_factor(db[i][2].real(), db[i][2].imag(), e.substrate_thickness, wl);
+                t1.fa = make_double2(fs.real(), fs.imag());
+            }
+        }
+        weights[size_t(b)] = run->weight;
+        if (b == 0) {
+            R.wl = wl;
+            R.cut = R.cuts[0];
+            R.db = db;
+        }
+    }
+    // pageable sources: staged before the calls return
+    CU(cudaMemcpyAsync(S->bmat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(S->bmat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(S->btab.p, tab.data(), tab.size() * sizeof(BatchTrans), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(S->bweight.p, weights.data(), weights.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    return run_schedule(R, src, 0.0);
 }
 
 }  // extern "C"

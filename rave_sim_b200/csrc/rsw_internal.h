@@ -76,6 +76,24 @@ enum PassFlags : int {
     PF_NOSTORE = 512, // column detection pass: bin the field only, do not write it
 };
 
+// Per-instance values of a batched pass: several sources with the same
+// field length and element geometry (the energies of one field length) run
+// in lockstep, each transform of the batch one instance. Only the values that
+// depend on the wavelength differ between instances.
+// Column pass: the transmission factors of the split step's element.
+struct BatchTrans {
+    double2 fa, fb;                         // grating / DBA / scalar factors
+    const double2 *mat_db, *mat_factor;     // sample: per-material tables of the instance
+    double sample_y;                        // sample: 2 pi dz / wl
+};
+// Row pass: the transfer function of the split step (chirp form).
+struct BatchProp {
+    double2 A;
+    double g_hi, g_lo;
+    const void *h3;
+    int64_t cut_lo, cut_hi;                 // used where PropArgs::has_cut
+};
+
 // Detector binning fused into the last inverse column pass of a phase step
 // (square_and_downsample, big-wave/propagation.py:279-320). Pixel j holds the
 // samples [bounds[j], bounds[j+1]) (np.histogram bins, built on the host);
@@ -92,6 +110,11 @@ struct DetectArgs {
     double *sum;             // n_pix raw sums
     unsigned *count;         // CTAs done
     double *acc, *comp;      // the phase step's accumulator row
+    // batched passes: instance b bins into sum + b * sum_stride and adds with
+    // weight bweight[b]; the instances are added in order (n_inst of them)
+    const double *bweight;
+    int64_t sum_stride;
+    int n_inst;
 };
 
 // Arguments of one pass. N = N1 * N2 samples; three-level plans split the
@@ -120,6 +143,10 @@ struct PassArgs {
     TransArgs tr;
     PropArgs pr;
     DetectArgs det;
+    // batched passes (NULL: one set of values for every transform):
+    // column pass, per instance of the batch; row pass, likewise
+    const BatchTrans *btr;
+    const BatchProp *bpr;
 };
 
 // Level structure of the internal spectrum layout (log2 lengths and digit

@@ -15,7 +15,11 @@ void count_launch() { ++g_launches; }
 
 cudaError_t launch_row_pass_f64(const PassArgs &a, int e, cudaStream_t s);
 cudaError_t launch_row_pass_f32(const PassArgs &a, int e, cudaStream_t s);
+cudaError_t launch_row_pass_f64_batch(const PassArgs &a, int e, cudaStream_t s);
+cudaError_t launch_row_pass_f32_batch(const PassArgs &a, int e, cudaStream_t s);
+// per-instance transfer functions take the batched kernels
 cudaError_t launch_row_pass(const PassArgs &a, bool dbl, int e, cudaStream_t s) {
+    if (a.bpr) return dbl ? launch_row_pass_f64_batch(a, e, s) : launch_row_pass_f32_batch(a, e, s);
     return dbl ? launch_row_pass_f64(a, e, s) : launch_row_pass_f32(a, e, s);
 }
 

@@ -105,7 +105,9 @@ static __device__ __noinline__ double2 sample_interp(const double2 *mat_db, doub
 
 // Sample row factor at sample n: exp(i y * np.interp(x, row_x, row_db, 0, 0))
 // (big-wave/optical_element.py:452-472). Returns false for vacuum (factor 1).
-__device__ __forceinline__ bool sample_factor(const TransArgs &t, int64_t n, double2 *f) {
+// The material tables and y are the instance's (t's own, or a batch entry's).
+__device__ __forceinline__ bool sample_factor(const TransArgs &t, const double2 *mat_db, const double2 *mat_factor,
+                                              double y, int64_t n, double2 *f) {
     const double x = __dmul_rn(double(n) - t.half_n, t.dx);
     const int64_t last = t.x_len - 1;
     const double x0 = sample_row_x(t, 0);
@@ -115,7 +117,7 @@ __device__ __forceinline__ bool sample_factor(const TransArgs &t, int64_t n, dou
     if (x == xl) {
         mi = t.row_grid[last];
         if (mi == 0) return false;
-        *f = t.mat_factor[mi];
+        *f = mat_factor[mi];
         return true;
     }
     int64_t j = int64_t(floor((x - x0) * t.sample_inv_psx));
@@ -128,11 +130,11 @@ __device__ __forceinline__ bool sample_factor(const TransArgs &t, int64_t n, dou
     const double xj = sample_row_x(t, j);
     if (m0 == m1 || x == xj) {
         if (m0 == 0) return false;
-        *f = t.mat_factor[m0];
+        *f = mat_factor[m0];
         return true;
     }
     // scalars by value: a reference to the kernel parameter would force it into local memory
-    *f = sample_interp(t.mat_db, t.psx, t.sample_xpos, t.sample_hw, t.sample_y, j, m0, m1, x, xj);
+    *f = sample_interp(mat_db, t.psx, t.sample_xpos, t.sample_hw, y, j, m0, m1, x, xj);
     return true;
 }
 
@@ -158,26 +160,36 @@ static __device__ __noinline__ double2 sample_interp(const double2 *mat_db, doub
 __device__ __forceinline__ double2 to_c(double2 a, double2) { return a; }
 __device__ __forceinline__ float2 to_c(double2 a, float2) { return make_float2(float(a.x), float(a.y)); }
 
+// u * f for a transmission factor with every rounding explicit (one product
+// rounded, one fused), so that every kernel variant that transmits (the
+// plain and the batched passes) rounds the same way
+__device__ __forceinline__ float2 tmul(float2 u, float2 f) {
+    return make_float2(__fmaf_rn(u.x, f.x, -__fmul_rn(u.y, f.y)), __fmaf_rn(u.x, f.y, __fmul_rn(u.y, f.x)));
+}
+__device__ __forceinline__ double2 tmul(double2 u, double2 f) {
+    return make_double2(__fma_rn(u.x, f.x, -__dmul_rn(u.y, f.y)), __fma_rn(u.x, f.y, __dmul_rn(u.y, f.x)));
+}
+
 template <typename Cx> __device__ __forceinline__ Cx apply_trans(const TransArgs &t, int64_t n, Cx u) {
     switch (t.kind) {
-    case TR_SCALAR: return cmul(u, to_c(t.fa, u));
+    case TR_SCALAR: return tmul(u, to_c(t.fa, u));
     case TR_GRATING: {
         const double x = grating_x(t, n);
         const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0);
-        return cmul(u, to_c(m ? t.fa : t.fb, u));
+        return tmul(u, to_c(m ? t.fa : t.fb, u));
     }
     case TR_DBA: {
         const double x = grating_x(t, n);
         const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0) &&
                        mod_less(x, t.pitch1, t.inv_pitch1, 0.0, t.dc1);
-        return cmul(u, to_c(m ? t.fa : t.fb, u));
+        return tmul(u, to_c(m ? t.fa : t.fb, u));
     }
     case TR_SAMPLE: {
         double2 f;
-        if (!sample_factor(t, n, &f)) return u;
+        if (!sample_factor(t, t.mat_db, t.mat_factor, t.sample_y, n, &f)) return u;
         // computed in FP64, stored in the field's precision
         const double2 ud = make_double2(double(u.x), double(u.y));
-        return to_c(cmul(ud, f), u);
+        return to_c(tmul(ud, f), u);
     }
     default: return u;
     }
@@ -196,7 +208,7 @@ __device__ __forceinline__ void apply_trans_e(const TransArgs &t, Pos pos, Cx *v
     case TR_SCALAR: {
         const Cx f = to_c(t.fa, Cx{});
 #pragma unroll
-        for (int r = 0; r < E; ++r) v[r] = cmul(v[r], f);
+        for (int r = 0; r < E; ++r) v[r] = tmul(v[r], f);
         break;
     }
     case TR_GRATING:
@@ -204,7 +216,7 @@ __device__ __forceinline__ void apply_trans_e(const TransArgs &t, Pos pos, Cx *v
         for (int r = 0; r < E; ++r) {
             const double x = grating_x(t, pos(r));
             const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0);
-            v[r] = cmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
+            v[r] = tmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
         }
         break;
     case TR_DBA:
@@ -213,19 +225,61 @@ __device__ __forceinline__ void apply_trans_e(const TransArgs &t, Pos pos, Cx *v
             const double x = grating_x(t, pos(r));
             const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0) &&
                            mod_less(x, t.pitch1, t.inv_pitch1, 0.0, t.dc1);
-            v[r] = cmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
+            v[r] = tmul(v[r], to_c(m ? t.fa : t.fb, Cx{}));
         }
         break;
     case TR_SAMPLE:
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             double2 f;
-            if (sample_factor(t, pos(r), &f)) {
+            if (sample_factor(t, t.mat_db, t.mat_factor, t.sample_y, pos(r), &f)) {
                 const double2 ud = make_double2(double(v[r].x), double(v[r].y));
-                v[r] = to_c(cmul(ud, f), Cx{});
+                v[r] = to_c(tmul(ud, f), Cx{});
             }
         }
         break;
+    default: break;
+    }
+}
+
+// apply_trans_e for one instance of a batched pass: the geometry from t, the
+// wavelength-dependent factors from the instance's entry b (loaded once per
+// tile, outside the unrolled samples)
+template <int E, typename Cx, typename Pos>
+__device__ __forceinline__ void apply_trans_batch(const TransArgs &t, const BatchTrans *__restrict__ b, Pos pos, Cx *v) {
+    switch (t.kind) {
+    case TR_SCALAR: {
+        const Cx f = to_c(__ldg(&b->fa), Cx{});
+#pragma unroll
+        for (int r = 0; r < E; ++r) v[r] = tmul(v[r], f);
+        break;
+    }
+    case TR_GRATING:
+    case TR_DBA: {
+        const Cx fa = to_c(__ldg(&b->fa), Cx{}), fb = to_c(__ldg(&b->fb), Cx{});
+        const bool dba = t.kind == TR_DBA;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const double x = grating_x(t, pos(r));
+            const bool m = mod_less(x, t.pitch0, t.inv_pitch0, t.half_dc0, t.dc0) &&
+                           (!dba || mod_less(x, t.pitch1, t.inv_pitch1, 0.0, t.dc1));
+            v[r] = tmul(v[r], m ? fa : fb);
+        }
+        break;
+    }
+    case TR_SAMPLE: {
+        const double2 *mdb = b->mat_db, *mf = b->mat_factor;
+        const double y = b->sample_y;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            double2 f;
+            if (sample_factor(t, mdb, mf, y, pos(r), &f)) {
+                const double2 ud = make_double2(double(v[r].x), double(v[r].y));
+                v[r] = to_c(tmul(ud, f), Cx{});
+            }
+        }
+        break;
+    }
     default: break;
     }
 }
@@ -349,8 +403,10 @@ template <typename Real, int LOG_L2, int E> constexpr int row_min_ctas() {
     return sizeof(Real) == 4 && LOG_L2 == 13 && E == 16 ? 2 : 1;
 }
 // TWF: the three-level variant with the W_{N2} twiddle before the forward
-// transform (a separate kernel, so that the two-level one carries no code for it)
-template <typename Real, int LOG_L2, int E, bool CHIRP, bool TWF = false>
+// transform (a separate kernel, so that the two-level one carries no code for it).
+// BATCH: the batched variant (per-instance transfer functions, a.bpr; chirp
+// form only), also a separate kernel so that the others carry no code for it.
+template <typename Real, int LOG_L2, int E, bool CHIRP, bool TWF = false, bool BATCH = false>
 __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Real, LOG_L2, E>()) row_pass_kernel(PassArgs a) {
     using B = Block<Real, LOG_L2, 1, E>;
     using Cx = typename B::Cx;
@@ -403,13 +459,22 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
             // taken once per row) and the register's part R[r] = exp(2 pi i g1 s_r),
             // s_r = freq_off(r) - L if the top frequency bit is set (all lanes read
             // the same R[r])
+            // (a batched pass takes G and A of the row's instance)
+            double g_hi = a.pr.g_hi, g_lo = a.pr.g_lo;
+            double2 A = a.pr.A;
+            if constexpr (BATCH) {
+                const BatchProp *bp = a.bpr + (row >> log_m);
+                g_hi = __ldg(&bp->g_hi);
+                g_lo = __ldg(&bp->g_lo);
+                A = __ldg(&bp->A);
+            }
             const double m = double(int64_t(1) << log_m);
-            const double gk = frac_dd(a.pr.g_hi, a.pr.g_lo, double(kbase * kbase));
-            const double g1h = 2.0 * m * a.pr.g_hi, g1l = 2.0 * m * a.pr.g_lo;
+            const double gk = frac_dd(g_hi, g_lo, double(kbase * kbase));
+            const double g1h = 2.0 * m * g_hi, g1l = 2.0 * m * g_lo;
             for (int idx = tp; idx < NCH; idx += B::NT) {
                 double2 w;
                 if (idx < 64) {
-                    w = cmul(a.pr.A, cis_turns(gk + frac_dd(g1h, g1l, double(kbase * idx))));
+                    w = cmul(A, cis_turns(gk + frac_dd(g1h, g1l, double(kbase * idx))));
                 } else if (idx < 64 + NQ) {
                     const int64_t b = int64_t(idx - 64) - NQ / 2;
                     w = cis_turns(frac_dd(g1h, g1l, double(kbase * 64 * b)));
@@ -491,15 +556,21 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
             // cutoff: k = kbase + k2 2^log_m in [cut_lo, cut_hi)  <=>  k2 in [k2lo, k2hi)
             int k2lo = 0, k2hi = 0;
             if (a.pr.has_cut) {
-                k2lo = k2_bound(a.pr.cut_lo - kbase, log_m, L);
-                k2hi = k2_bound(a.pr.cut_hi - kbase, log_m, L);
+                if constexpr (BATCH) {
+                    const BatchProp *bp = a.bpr + (row >> log_m);
+                    k2lo = k2_bound(__ldg(&bp->cut_lo) - kbase, log_m, L);
+                    k2hi = k2_bound(__ldg(&bp->cut_hi) - kbase, log_m, L);
+                } else {
+                    k2lo = k2_bound(a.pr.cut_lo - kbase, log_m, L);
+                    k2hi = k2_bound(a.pr.cut_hi - kbase, log_m, L);
+                }
             }
             const unsigned cut_span = unsigned(k2hi - k2lo);
             if (a.pr.has_h) {
                 // H = P[fbase & 63] * Q[fbase >> 6] * R[r] * h3[r][tp]; k2 >= L/2
                 // (k2s = k2 - L) is decided by the compile-time part of the
                 // frequency, so 0 <= fbase < L/2
-                const Lf *h3 = static_cast<const Lf *>(a.pr.h3);
+                const Lf *h3 = static_cast<const Lf *>(BATCH ? a.bpr[row >> log_m].h3 : a.pr.h3);
                 if constexpr (B::LIFT) {
                     // three rotations: the thread's P Q (FP64 product), R[r], h3
                     const double2 *chd = reinterpret_cast<const double2 *>(chp);
@@ -598,14 +669,14 @@ __device__ __forceinline__ int64_t pixel_of(const DetectArgs &d, int64_t n) {
 // rows; a group of G = min(C, 32) lanes whose samples share a pixel adds its
 // group sum with one atomic, otherwise each lane adds its own.
 template <typename B, typename Cx>
-__device__ __forceinline__ void detect_bin(const DetectArgs &d, int64_t base, int64_t col, int tp, const Cx *v,
+__device__ __forceinline__ void detect_bin(const DetectArgs &d, double *sum, int64_t col, int tp, const Cx *v,
                                            int log_n2) {
     constexpr int C = B::NT / B::T, G = C < 32 ? C : 32;
     const unsigned lane = threadIdx.x & 31u;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~unsigned(G - 1));
 #pragma unroll
     for (int r = 0; r < B::E; ++r) {
-        const int64_t n = base + (int64_t(B::first_pos(tp, r)) << log_n2) + col;
+        const int64_t n = (int64_t(B::first_pos(tp, r)) << log_n2) + col;
         const bool in = n >= d.lo && n < d.hi;
         if (!__any_sync(0xffffffffu, in)) continue;
         int64_t j = -1;
@@ -621,9 +692,9 @@ __device__ __forceinline__ void detect_bin(const DetectArgs &d, int64_t base, in
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o, G);
         if (uniform) {
-            if ((lane & unsigned(G - 1)) == 0 && lead >= 0) atomicAdd(d.sum + lead, g);
+            if ((lane & unsigned(G - 1)) == 0 && lead >= 0) atomicAdd(sum + lead, g);
         } else if (j >= 0) {
-            atomicAdd(d.sum + j, s);
+            atomicAdd(sum + j, s);
         }
     }
 }
@@ -631,7 +702,9 @@ __device__ __forceinline__ void detect_bin(const DetectArgs &d, int64_t base, in
 // End of a detection pass: the CTA that finishes last turns the sums into
 // the pixel values of square_and_downsample, (((sum cos_j) dx) psy) / r_j,
 // adds weight * value into the accumulator with Kahan compensation, and
-// zeroes the sums and the count for the next pass.
+// zeroes the sums and the count for the next pass. A batched pass adds its
+// instances one after the other, in instance order: the order in which
+// separate runs of the same sources would add them.
 __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
     __shared__ int last;
     __threadfence();  // this thread's atomics before the count
@@ -641,13 +714,21 @@ __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
     if (!last) return;
     __threadfence();
     for (int64_t j = threadIdx.x; j < d.n_pix; j += blockDim.x) {
-        const double s = __ldcg(d.sum + j);
-        const double val = (((s * __ldg(d.cosv + j)) * d.dx) * d.psy) / __ldg(d.rv + j);
-        const double y = __dsub_rn(__dmul_rn(d.weight, val), d.comp[j]);
-        const double t = __dadd_rn(d.acc[j], y);
-        d.comp[j] = __dsub_rn(__dsub_rn(t, d.acc[j]), y);
-        d.acc[j] = t;
-        d.sum[j] = 0.0;
+        const double cj = __ldg(d.cosv + j), rj = __ldg(d.rv + j);
+        double acc = d.acc[j], comp = d.comp[j];
+        for (int b = 0; b < d.n_inst; ++b) {
+            double *sum = d.sum + b * d.sum_stride + j;
+            const double s = __ldcg(sum);
+            const double val = (((s * cj) * d.dx) * d.psy) / rj;
+            const double w = d.bweight ? __ldg(d.bweight + b) : d.weight;
+            const double y = __dsub_rn(__dmul_rn(w, val), comp);
+            const double t = __dadd_rn(acc, y);
+            comp = __dsub_rn(__dsub_rn(t, acc), y);
+            acc = t;
+            *sum = 0.0;
+        }
+        d.acc[j] = acc;
+        d.comp[j] = comp;
     }
     if (threadIdx.x == 0) *d.count = 0u;
 }
@@ -656,7 +737,8 @@ __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
 // step: each CTA takes a contiguous range of tiles (adjacent columns), bins
 // |u|^2 after the inverse transform (detect_bin) and stores the field unless
 // PF_NOSTORE; the last CTA finishes the detector row (detect_finish).
-template <typename Real, int LOG_L1, int C, int E, bool DET = false>
+// BATCH: per-instance transmission factors (a.btr), a separate kernel
+template <typename Real, int LOG_L1, int C, int E, bool DET = false, bool BATCH = false>
 __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(PassArgs a) {
     using B = Block<Real, LOG_L1, C, E>;
     using Cx = typename B::Cx;
@@ -757,8 +839,15 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
                 v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[int64_t(B::first_pos(tp, r)) << log_n2];
         }
         // the detection variant runs the inverse only: no transmission, no forward
-        if (!DET && (flags & PF_TRANS))
-            apply_trans_e<E>(a.tr, [&](int r) { return base + (int64_t(B::first_pos(tp, r)) << log_n2) + col; }, v);
+        // (single-transform passes transmit at base 0; a batched pass at the
+        // position within the tile's own transform)
+        if (!DET && (flags & PF_TRANS)) {
+            if constexpr (BATCH)
+                apply_trans_batch<E>(a.tr, a.btr + batch,
+                                     [&](int r) { return (int64_t(B::first_pos(tp, r)) << log_n2) + col; }, v);
+            else
+                apply_trans_e<E>(a.tr, [&](int r) { return base + (int64_t(B::first_pos(tp, r)) << log_n2) + col; }, v);
+        }
         if (!DET && (flags & PF_FWD)) {
             B::forward(sm, tp, v, tw);
             if (flags & PF_TW) {
@@ -778,7 +867,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r) gout[int64_t(B::last_pos(tp, r)) << log_n2] = v[r];
         } else {
-            if constexpr (DET) detect_bin<B>(a.det, base, col, tp, v, log_n2);
+            if constexpr (DET) detect_bin<B>(a.det, a.det.sum + batch * a.det.sum_stride, col, tp, v, log_n2);
             if (!DET || !(flags & PF_NOSTORE)) {
 #pragma unroll
                 for (int r = 0; r < E; ++r) gout[int64_t(B::first_pos(tp, r)) << log_n2] = v[r];
@@ -850,9 +939,10 @@ static const LaunchSetup *launch_setup(K kernel, int threads, size_t smem, size_
 template <int L> constexpr int n_vec() { return 64 + ((L >> 6) > 0 ? (L >> 6) : 1); }
 template <int L, int E> constexpr int n_chirp() { return 64 + ((L >> 6) > 1 ? (L >> 6) : 2) + E; }
 
-template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
+template <typename Real, int LG, int E, bool CH, bool TWF, bool BT>
+static cudaError_t row_launch(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, 1, E>;
-    auto k = row_pass_kernel<Real, LG, E, CH, TWF>;
+    auto k = row_pass_kernel<Real, LG, E, CH, TWF, BT>;
     const size_t smem = (B::SMEM + 15) / 16 * 16 + 2 * size_t(n_vec<B::L>() + n_chirp<B::L, E>()) * 16;
     static LaunchSetup setup[LAUNCH_MAX_DEVICES];
     static std::once_flag once[LAUNCH_MAX_DEVICES];
@@ -868,12 +958,18 @@ template <typename Real, int LG, int E, bool CH, bool TWF> static cudaError_t ro
 // PF_TWF (rows of three-level plans) takes the TWF variant, for the chirp
 // form and for the per-sample transfer function (exact kernel) alike; rows of
 // multi-level plans hold at least 2^7 samples
-template <typename Real, int LG, int E, bool CH> static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
-    if constexpr (LG >= 7) {
-        if (a.flags & PF_TWF) return row_launch<Real, LG, E, CH, true>(a, s);
+// BT: the batched variant, chirp form only
+template <typename Real, int LG, int E, bool CH, bool BT = false>
+static cudaError_t row_impl(const PassArgs &a, cudaStream_t s) {
+    if constexpr (BT && !CH) {
+        return cudaErrorInvalidValue;
+    } else {
+        if constexpr (LG >= 7) {
+            if (a.flags & PF_TWF) return row_launch<Real, LG, E, CH, true, BT>(a, s);
+        }
+        if (a.flags & PF_TWF) return cudaErrorInvalidValue;
+        return row_launch<Real, LG, E, CH, false, BT>(a, s);
     }
-    if (a.flags & PF_TWF) return cudaErrorInvalidValue;
-    return row_launch<Real, LG, E, CH, false>(a, s);
 }
 
 // Columns per CTA of the column kernel (16 samples per thread): enough for
@@ -886,10 +982,10 @@ constexpr int col_c(int log_l) {
 // segments, measured 26 % and 13 % faster than 32-byte ones at 2^28 and 2^24)
 constexpr int col_c64(int log_l) { return log_l == 10 ? 16 : log_l == 11 ? 8 : col_c(log_l); }
 
-template <typename Real, int LG, int C, int E, bool DET = false>
+template <typename Real, int LG, int C, int E, bool DET = false, bool BT = false>
 static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
-    auto k = col_pass_kernel<Real, LG, C, E, DET>;
+    auto k = col_pass_kernel<Real, LG, C, E, DET, BT>;
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
     const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, 16>();

@@ -354,8 +354,37 @@ class Simulation:
 
         ``source``: {type: plane, z} | {type: point, x, z} | {type: vector, z}
         with ``field`` a host numpy array or CUDA tensor of N samples."""
-        src = L.Source()
         keep = []
+        src = self._source(source, field, keep)
+        run = self._run(energy, db_table, weight, wavelength, keep)
+        L.check(self._lib.rsw_sim_run(self._h, C.byref(src), C.byref(run), _stream_ptr()))
+
+    def run_sources(self, runs: Sequence[dict], *, source: dict, field=None):
+        """Run several sources of the same geometry in lockstep
+        (rsw_sim_run_batch): ``runs`` holds one dict per source with
+        ``energy``, ``db_table`` and optional ``weight`` (1.0) and
+        ``wavelength``; the detector values are added in list order, as
+        run_source calls in that order would add them."""
+        keep = []
+        src = self._source(source, field, keep)
+        arr = (L.SourceRun * max(len(runs), 1))()
+        for i, r in enumerate(runs):
+            arr[i] = self._run(r["energy"], r["db_table"], r.get("weight", 1.0), r.get("wavelength"), keep)
+        L.check(self._lib.rsw_sim_run_batch(self._h, C.byref(src), arr, len(runs), _stream_ptr()))
+
+    def _run(self, energy, db_table, weight, wavelength, keep):
+        db = self.deltabeta_vector(db_table)
+        keep.append(db)
+        run = L.SourceRun()
+        run.energy_ev = float(energy)
+        run.deltabeta = db.view(np.float64).ctypes.data_as(L._DP) if db.size else None
+        run.n_deltabeta = db.size
+        run.weight = float(weight)
+        run.wavelength_m = float(wavelength) if wavelength is not None else 0.0
+        return run
+
+    def _source(self, source: dict, field, keep):
+        src = L.Source()
         t = source["type"]
         src.z = float(source.get("z", 0.0))
         if t == "plane":
@@ -382,15 +411,7 @@ class Simulation:
                 src.h_field = f.ctypes.data
         else:
             raise ValueError(f"unknown source type {t!r}")
-        db = self.deltabeta_vector(db_table)
-        keep.append(db)
-        run = L.SourceRun()
-        run.energy_ev = float(energy)
-        run.deltabeta = db.view(np.float64).ctypes.data_as(L._DP) if db.size else None
-        run.n_deltabeta = db.size
-        run.weight = float(weight)
-        run.wavelength_m = float(wavelength) if wavelength is not None else 0.0
-        L.check(self._lib.rsw_sim_run(self._h, C.byref(src), C.byref(run), _stream_ptr()))
+        return src
 
     def detected(self) -> np.ndarray:
         """The FP64 accumulator as (nr_phase_steps, n_pix); synchronises."""
