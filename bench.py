@@ -457,14 +457,17 @@ def main():
     n = gd["n"]
     sim = gd["sim"]
     sim.set_timing(True)
+    steps0 = sim.split_steps
     if batch:
         sim.run_sources([{"energy": e, "db_table": gd["db"](e), "weight": 0.0} for e in gd["energies"]],
                         source=gd["case"]["source"])
-        per_launch = len(gd["energies"])  # fields per pass launch
     else:
         e = gd["energies"][0]
         sim.run_source(energy=e, db_table=gd["db"](e), source=gd["case"]["source"], weight=0.0)
-        per_launch = 1
+    # fields per pass launch: split steps of all sources over row launches (a
+    # batch that the engine runs source by source launches once per field)
+    row_t, row_n = sim.timing(0)
+    per_launch = max(1, int(round((sim.split_steps - steps0) / row_n))) if row_n else 1
     kinds = {}
     for k, name in ((0, "row_pass"), (1, "col_pass"), (2, "detect"), (3, "mid_pass")):
         t, cnt = sim.timing(k)
@@ -489,6 +492,13 @@ def main():
         roofline["traffic"] *= per_launch
         roofline["traffic_source"] += f", times the {per_launch} fields of a batched launch"
     roofline["fields_per_launch"] = per_launch
+    if not batch or len(gd["energies"]) == 1:
+        sources_mode = "one source after the other"
+    elif per_launch > 1:
+        sources_mode = "lockstep batch per field length (one launch per pass for all its energies)"
+    else:
+        sources_mode = ("one source after the other (the engine's choice for this plan: its batched kernels "
+                        "hold fewer CTAs per SM)")
 
     # ---- mixed precision against the complex128 run of the same step
     precision = None
@@ -531,8 +541,7 @@ def main():
                "l2_policy": "inputs larger than L2" if n * s_bytes > (126 << 20) else
                             "field smaller than L2 (no flush)",
                "parallelism": f"dp{ws} (energies sharded, detector all-reduce)",
-               "sources": "lockstep batch per field length (one launch per pass for all its energies)"
-                          if batch else "one source after the other",
+               "sources": sources_mode,
                "schedule": {"autotuned": tuning} if tuning else "built-in"}
         if args.workload == "talbot_lau":
             cfg.update({"n": n, "energies_per_rank": len(gd["energies"]), "field_bytes": n * s_bytes,

@@ -2479,6 +2479,29 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     return run_schedule(R, src, run->weight);
 }
 
+}  // extern "C"
+
+// Whether the batched column kernel of the plan's transmitting pass holds as
+// many CTAs per SM as the plain one. Its per-instance factors take registers
+// that the plain kernel does not need; where that costs resident CTAs (some
+// complex128 column shapes of 64 to 256 threads), a batch is slower than the
+// same sources one after the other (2^26 complex128, three levels with
+// columns of 2^7: 24.1 against 27.5 G samples*steps/s on B200).
+static bool batch_keeps_occupancy(const rsw_plan_s *P) {
+    PassArgs a = base_args(P);
+    a.flags = PF_FWD | PF_INV | PF_TW | PF_TRANS | (P->three() ? PF_TWI : 0);
+    int64_t plain = 0, batched = 0;
+    a.resident = &plain;
+    if (launch_col_pass(a, P->dbl(), P->col_e, nullptr) != cudaSuccess) return false;
+    BatchTrans dummy{};
+    a.btr = &dummy;
+    a.resident = &batched;
+    if (launch_col_pass(a, P->dbl(), P->col_e, nullptr) != cudaSuccess) return false;
+    return batched >= plain;
+}
+
+extern "C" {
+
 rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
                              void *stream) {
     if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
@@ -2492,7 +2515,8 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
     // Fresnel kernel and the fused detection; everything else runs the
     // sources one after the other, with the same results
     const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
-                          S->hist_dz == 0.0 && S->keypoints.empty() && !S->els.empty() && S->geom.n_pix > 0;
+                          S->hist_dz == 0.0 && S->keypoints.empty() && !S->els.empty() && S->geom.n_pix > 0 &&
+                          batch_keeps_occupancy(P);
     if (!lockstep) {
         for (int64_t b = 0; b < count; ++b) CHECK(rsw_sim_run(S, src, runs + b, stream));
         return RSW_OK;

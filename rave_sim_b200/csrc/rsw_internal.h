@@ -147,6 +147,9 @@ struct PassArgs {
     // column pass, per instance of the batch; row pass, likewise
     const BatchTrans *btr;
     const BatchProp *bpr;
+    // column pass: when set, the launch functions store the kernel's resident
+    // CTAs on the current device here and launch nothing
+    int64_t *resident;
 };
 
 // Level structure of the internal spectrum layout (log2 lengths and digit

@@ -571,32 +571,43 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                 // (k2s = k2 - L) is decided by the compile-time part of the
                 // frequency, so 0 <= fbase < L/2
                 const Lf *h3 = static_cast<const Lf *>(BATCH ? a.bpr[row >> log_m].h3 : a.pr.h3);
+                // rows without cut frequencies (cut_span 0, uniform per row)
+                // take the loop without the per-sample test
+                const auto zero_cut = [&](int r, Cx x) {
+                    return unsigned((fbase | B::freq_off(r)) - k2lo) < cut_span ? Cx{} : x;
+                };
                 if constexpr (B::LIFT) {
                     // three rotations: the thread's P Q (FP64 product), R[r], h3
                     const double2 *chd = reinterpret_cast<const double2 *>(chp);
                     const Lf tl = lift_of(cmul(chd[fbase & 63], chd[64 + (fbase >> 6) + NQ / 2]));
+                    const auto rotate = [&](auto cut) {
 #pragma unroll
-                    for (int r = 0; r < E; ++r) {
-                        const int k2 = fbase | B::freq_off(r);
-                        const Lf rr = chp[64 + NQ + r], g = __ldg(h3 + r * B::T + tp);
-                        Cx x = cscale(v[r], tl.z * rr.z * g.z);
-                        x = lift(lift(lift(x, tl.x, tl.y), rr.x, rr.y), g.x, g.y);
-                        v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : x;
-                        if (r % 4 == 3) asm volatile("" ::: "memory");
-                    }
+                        for (int r = 0; r < E; ++r) {
+                            const Lf rr = chp[64 + NQ + r], g = __ldg(h3 + r * B::T + tp);
+                            Cx x = cscale(v[r], tl.z * rr.z * g.z);
+                            x = lift(lift(lift(x, tl.x, tl.y), rr.x, rr.y), g.x, g.y);
+                            v[r] = decltype(cut)::value ? zero_cut(r, x) : x;
+                            if (r % 4 == 3) asm volatile("" ::: "memory");
+                        }
+                    };
+                    if (cut_span == 0) rotate(std::false_type{});
+                    else rotate(std::true_type{});
                 } else {
                 const Cx tb = cmul(chp[fbase & 63], chp[64 + (fbase >> 6) + NQ / 2]);
+                const auto multiply = [&](auto cut) {
 #pragma unroll
-                for (int r = 0; r < E; ++r) {
-                    const int k2 = fbase | B::freq_off(r);
-                    const Cx h = cmul(cmul(tb, chp[64 + NQ + r]), __ldg(h3 + r * B::T + tp));
-                    v[r] = unsigned(k2 - k2lo) < cut_span ? Cx{} : cmul(v[r], h);
-                    // a compiler-only barrier per 4 samples: without it all E
-                    // h3 loads were issued ahead and held live (the 2^14
-                    // complex64 row spilled 132 bytes per thread instead of 52,
-                    // 5 % slower)
-                    if (r % 4 == 3) asm volatile("" ::: "memory");
-                }
+                    for (int r = 0; r < E; ++r) {
+                        const Cx h = cmul(cmul(tb, chp[64 + NQ + r]), __ldg(h3 + r * B::T + tp));
+                        v[r] = decltype(cut)::value ? zero_cut(r, cmul(v[r], h)) : cmul(v[r], h);
+                        // a compiler-only barrier per 4 samples: without it all E
+                        // h3 loads were issued ahead and held live (the 2^14
+                        // complex64 row spilled 132 bytes per thread instead of 52,
+                        // 5 % slower)
+                        if (r % 4 == 3) asm volatile("" ::: "memory");
+                    }
+                };
+                if (cut_span == 0) multiply(std::false_type{});
+                else multiply(std::true_type{});
                 }
             } else {
 #pragma unroll
@@ -737,7 +748,10 @@ __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
 // step: each CTA takes a contiguous range of tiles (adjacent columns), bins
 // |u|^2 after the inverse transform (detect_bin) and stores the field unless
 // PF_NOSTORE; the last CTA finishes the detector row (detect_finish).
-// BATCH: per-instance transmission factors (a.btr), a separate kernel
+// BATCH: per-instance transmission factors (a.btr), a separate kernel. Its
+// factors live in registers where the plain kernel reads them from the
+// parameter bank, so some complex128 shapes hold fewer CTAs per SM
+// (col_resident; the host then runs such sources one after the other).
 template <typename Real, int LOG_L1, int C, int E, bool DET = false, bool BATCH = false>
 __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(PassArgs a) {
     using B = Block<Real, LOG_L1, C, E>;
@@ -996,6 +1010,10 @@ static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     if (st->attr != cudaSuccess) return st->attr;
     const bool tables = a.flags & (PF_TW | PF_TWI);
     const int64_t cap = tables ? st->cap[0] : st->cap[1];
+    if (a.resident) {  // a query: the resident CTAs per device, no launch
+        *a.resident = cap;
+        return cudaSuccess;
+    }
     const int64_t tiles = (a.n >> LG) / C;
     if ((int64_t(1) << a.log_n2) < C) return cudaErrorInvalidValue;  // fewer columns per batch than a tile
     int64_t grid = tiles < cap ? tiles : cap;

@@ -8,7 +8,8 @@ order of the atomic per-pixel sums of the fused detection differs. Tolerance
 are held to.
 
 Cases: the three-grating interferometer (gratings, phase stepping) in both
-dtypes, with each instance checked alone through one-hot weights; a sample
+dtypes, with each instance checked alone through one-hot weights and the
+complex64 batch checked to launch one kernel per pass for all instances; a sample
 (int8 grid, per-energy material tables) with a cutoff angle that is active
 for some energies only; a point source; a forced three-level plan; batches
 that grow the sim's batch buffers; the configurations that run one source
@@ -66,8 +67,11 @@ def test_interferometer_batch_equals_runs(dtype):
         l2 = lib.rsw_launch_count()
         assert seq.shape == (4, 100)
         assert rel_l2(bat, seq) < TOL
-        # one launch per pass for all instances
-        assert (l2 - l1) * 3 < (l1 - l0)
+        # one launch per pass for all instances (complex64 column kernels
+        # keep their occupancy when batched; complex128 shapes that would not
+        # run the sources one after the other)
+        if dtype == "c8":
+            assert (l2 - l1) * 3 < (l1 - l0)
         # every instance alone: one-hot weights against its own run
         for b, e in enumerate(ENERGIES):
             one = [dict(r, weight=1.0 if i == b else 0.0) for i, r in enumerate(runs)]
