@@ -313,8 +313,9 @@ rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run 
  * add them. The sim keeps batch buffers of count * N samples (two with phase
  * stepping), sized for the largest batch run so far. Lockstep needs a plan
  * of two or three levels, the Fresnel propagator, no history, no keypoints,
- * at least one element and a detector of at least one pixel; otherwise the
- * sources run one after the other through rsw_sim_run. A batch keeps no
+ * at least one element and a detector of at least one pixel, and no final
+ * fields (rsw_sim_set_final_fields); otherwise the sources run one after the
+ * other through rsw_sim_run. A batch keeps no
  * final field (rsw_sim_final_field). count <= RSW_BATCH_MAX. */
 #define RSW_BATCH_MAX 4096
 rsw_status rsw_sim_run_batch(rsw_sim sim, const rsw_source *src, const rsw_source_run *runs,
@@ -368,6 +369,16 @@ rsw_status rsw_sim_history(rsw_sim sim, double *h_history, double *h_z, int64_t 
  * keypoint costs one copy, or one inverse column pass where the field is held
  * in the passes' intermediate order. */
 rsw_status rsw_sim_set_keypoints(rsw_sim sim, void *const *dst, int64_t n_dst);
+/* Final fields of every phase step (replaces big-wave's save_u with
+ * save_final_u_vectors, wavesim.py:58-82, called after each phase step at
+ * :221-227 and :288-294): during each following run, the field at the
+ * detector plane of phase step p is written in natural order to dst[p]. dst
+ * holds n_dst = nr_phase_steps device buffers of N samples of the
+ * simulation's dtype on its device (NULL entries are skipped); the pointers
+ * are kept until the next call, and n_dst = 0 turns it off. The field is
+ * written by the phase step's last pass, which then stores it instead of only
+ * binning it. */
+rsw_status rsw_sim_set_final_fields(rsw_sim sim, void *const *dst, int64_t n_dst);
 
 #ifdef __cplusplus
 }

@@ -138,6 +138,7 @@ SIGNATURES = {
     "rsw_plan_set_propagator": (C.c_int, [_P, C.c_int]),
     "rsw_sim_history": (C.c_int, [_P, _DP, _DP, C.POINTER(_I64), _P]),
     "rsw_sim_set_keypoints": (C.c_int, [_P, C.POINTER(C.c_void_p), _I64]),
+    "rsw_sim_set_final_fields": (C.c_int, [_P, C.POINTER(C.c_void_p), _I64]),
     "rsw_sim_create": (C.c_int, [C.POINTER(_P), C.POINTER(SimDesc)]),
     "rsw_sim_destroy": (C.c_int, [_P]),
     "rsw_sim_shape": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),

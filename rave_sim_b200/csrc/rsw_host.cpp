@@ -1656,6 +1656,9 @@ struct rsw_sim_s {
     // keypoints (big-wave/wavesim.py:35-55): caller buffers for the field
     // before / after each element of the first pass, NULL entries skipped
     std::vector<void *> keypoints;
+    // final fields (big-wave's save_u): caller buffers for the field at the
+    // detector of each phase step, NULL entries skipped
+    std::vector<void *> final_fields;
     // lockstep batches (rsw_sim_run_batch), sized for the largest batch so far:
     // field buffers of nb * N samples, per-instance transmission entries
     // [element][grating, substrate][instance], sample material tables
@@ -1964,16 +1967,19 @@ struct Runner {
     // where the field is not in the multi-level "mid" representation.
     rsw_status finish_phase(int64_t phase, double weight, bool keep) {
         const int64_t np = S->geom.n_pix;
+        // the caller's buffer for this phase step's final field, if any
+        void *fin = size_t(phase) < S->final_fields.size() ? S->final_fields[size_t(phase)] : nullptr;
         if (!(mid && P->log_n1 > 0 && np > 0)) {
             CHECK(finalize());
+            if (fin) CU(cudaMemcpyAsync(fin, bp(cur), size_t(P->n) * P->elem(), cudaMemcpyDeviceToDevice, st));
             return detect(phase, weight);
         }
         const int dst = target();
         PassArgs a = base_args(P);
         a.n = P->n * nb;
         a.in = bp(cur);
-        a.out = bp(dst);
-        a.flags = col_inv(P) | (keep ? 0 : PF_NOSTORE);
+        a.out = fin && !keep ? fin : bp(dst);
+        a.flags = col_inv(P) | (keep || fin ? 0 : PF_NOSTORE);
         DetectArgs &d = a.det;
         d.bounds = (const int64_t *)S->bounds.p;
         d.cosv = (const double *)S->cosv.p;
@@ -2004,6 +2010,7 @@ struct Runner {
         if (keep) {
             cur = dst;
             mid = false;
+            if (fin) CU(cudaMemcpyAsync(fin, bp(cur), size_t(P->n) * P->elem(), cudaMemcpyDeviceToDevice, st));
         }
         return RSW_OK;
     }
@@ -2280,6 +2287,19 @@ rsw_status rsw_sim_set_keypoints(rsw_sim S, void *const *dst, int64_t n_dst) {
     return RSW_OK;
 }
 
+rsw_status rsw_sim_set_final_fields(rsw_sim S, void *const *dst, int64_t n_dst) {
+    if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
+    if (n_dst == 0) {
+        S->final_fields.clear();
+        return RSW_OK;
+    }
+    if (!dst || n_dst != S->nr_phase_steps)
+        return fail(RSW_ERR_INVALID, "final fields: %lld buffers for %lld phase steps", (long long)n_dst,
+                    (long long)S->nr_phase_steps);
+    S->final_fields.assign(dst, dst + n_dst);
+    return RSW_OK;
+}
+
 rsw_status rsw_sim_history(rsw_sim S, double *h_out, double *h_z, int64_t *n_entries, void *stream) {
     if (!S) return fail(RSW_ERR_INVALID, "sim is NULL");
     const int64_t n = int64_t(S->hist_z.size()), np = S->geom.n_pix;
@@ -2515,8 +2535,8 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
     // Fresnel kernel and the fused detection; everything else runs the
     // sources one after the other, with the same results
     const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
-                          S->hist_dz == 0.0 && S->keypoints.empty() && !S->els.empty() && S->geom.n_pix > 0 &&
-                          batch_keeps_occupancy(P);
+                          S->hist_dz == 0.0 && S->keypoints.empty() && S->final_fields.empty() &&
+                          !S->els.empty() && S->geom.n_pix > 0 && batch_keeps_occupancy(P);
     if (!lockstep) {
         for (int64_t b = 0; b < count; ++b) CHECK(rsw_sim_run(S, src, runs + b, stream));
         return RSW_OK;

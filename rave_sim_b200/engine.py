@@ -480,6 +480,28 @@ class Simulation:
             raise ValueError("keypoints are off (set_keypoints(True) before the run)")
         return list(self._kp)
 
+    def set_final_fields(self, enable: bool):
+        """Keep the field at the detector of every phase step of the
+        following runs (big-wave's save_u with save_final_u_vectors,
+        wavesim.py:58-82) in device buffers; ``final_fields()`` returns them."""
+        if not enable:
+            L.check(self._lib.rsw_sim_set_final_fields(self._h, None, 0))
+            self._ff = None
+            return
+        torch = _torch()
+        k = self.nr_phase_steps
+        bufs = [torch.empty(self.n, dtype=torch_dtype(self.code), device="cuda") for _ in range(k)]
+        ptrs = (C.c_void_p * k)(*[_dptr(b) for b in bufs])
+        L.check(self._lib.rsw_sim_set_final_fields(self._h, ptrs, k))
+        self._ff = bufs
+
+    def final_fields(self):
+        """Final field of each phase step of the last run (u_0000, u_0001, ...
+        of big-wave): CUDA tensors of N samples."""
+        if getattr(self, "_ff", None) is None:
+            raise ValueError("final fields are off (set_final_fields(True) before the run)")
+        return list(self._ff)
+
     def timing(self, kind: int):
         ms, n = C.c_double(), C.c_int64()
         L.check(self._lib.rsw_sim_timing(self._h, int(kind), C.byref(ms), C.byref(n)))

@@ -11,8 +11,9 @@ The directory layout is the reference's (big-wave/Readme.md, written by
 
 ``run_single_simulation`` mirrors ``multisim.run_single_simulation``
 (big-wave/multisim.py:50-150): it writes ``NNNNNNNN/detected.npy`` (float64,
-shape (nr_phase_steps, nr_pixels)) and, with ``save_final_u_vectors`` and no
-phase stepping, ``NNNNNNNN/u_0000.npy``. The command line mirrors fast-wave's
+shape (nr_phase_steps, nr_pixels)) and, with ``save_final_u_vectors``, the
+field at the detector of each phase step as ``NNNNNNNN/u_{step:04}.npy``
+(big-wave/wavesim.py:58-82). The command line mirrors fast-wave's
 ``fastwave <sim_dir> -s <idx>`` (fast-wave/main.cpp:18-57):
 
     python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16] [--history_dz DZ]
@@ -130,6 +131,8 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, save_keypo
         sim.set_history(history_dz)
         if save_keypoints_path is not None:
             sim.set_keypoints(True)
+        if c["save_final_u_vectors"]:
+            sim.set_final_fields(True)
         sim.reset()
         sim.run_source(energy=c["energy"], db_table=c["db"], source=c["source"], field=field)
         det = sim.detected()
@@ -147,9 +150,8 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, save_keypo
                     detector_x_vector(sp["detector_size"], sp["detector_pixel_size_x"]))
         np.save(out_dir / "detected.npy", det)
         if c["save_final_u_vectors"]:
-            if det.shape[0] != 1:
-                raise ValueError("save_final_u_vectors with phase stepping is not supported")
-            np.save(out_dir / "u_0000.npy", sim.final_field().cpu().numpy())
+            for step, u in enumerate(sim.final_fields()):
+                np.save(out_dir / f"u_{step:04}.npy", u.cpu().numpy())
         return det
     finally:
         sim.close()

@@ -92,3 +92,50 @@ def test_simdir_keypoints(tmp_path):
     kps = np.stack([np.load(kp / f) for f in files])
     assert kps.dtype == np.complex128 and kps.shape[1] == case["sim_params"]["N"]
     assert rel_l2(kps[:, ::int(d["keypoints_stride"])], d["keypoints_sub"]) < 1e-10
+
+
+# ---------------------------------------------------------------- final fields
+# big-wave's save_u (wavesim.py:58-82) with save_final_u_vectors writes the
+# field at the detector after every phase step (u_0000.npy, u_0001.npy, ...).
+@pytest.mark.parametrize("name", ["sample_stepped", "tl3g_point_phase"])
+@pytest.mark.parametrize("dtype,tol", [("c16", 1e-13), ("c8", 1e-6)])
+def test_final_field_of_every_phase_step(name, dtype, tol):
+    case, grids, d = load_case(name)
+    sim = rsw.Simulation(case, grids=grids, dtype=dtype, cutoff_angles=case["cutoff_angles"])
+    try:
+        sim.set_final_fields(True)
+        sim.reset()
+        sim.run_source(energy=case["energy"], db_table=case["db"], source=case["source"])
+        det = sim.detected()
+        fields = [f.cpu().numpy().astype(np.complex128) for f in sim.final_fields()]
+        last = sim.final_field().cpu().numpy().astype(np.complex128)
+    finally:
+        sim.close()
+    assert len(fields) == det.shape[0] > 1
+    ref = bw.make_sim(case)
+    for p, u in enumerate(fields):
+        # each field bins to its own phase step's detector row
+        assert rel_l2(bw.square_and_downsample(u, ref, ref.z_detector), det[p]) < tol, p
+    assert rel_l2(fields[0], fields[1]) > 1e-6  # the stepped element moved
+    assert np.array_equal(fields[-1], last)
+
+
+def test_simdir_writes_the_final_field_of_every_phase_step(tmp_path):
+    case, grids, d = load_case("tl3g_point_phase")
+    import yaml
+
+    cfg = {"sim_params": case["sim_params"], "use_disk_vector": False, "save_final_u_vectors": True,
+           "dtype": "c16", "elements": case["elements"]}
+    (tmp_path / "config.yaml").write_text(yaml.safe_dump(cfg))
+    (tmp_path / "computed.yaml").write_text(yaml.safe_dump({"cutoff_angles": case["cutoff_angles"]}))
+    sub = tmp_path / "00000000"
+    sub.mkdir()
+    (sub / "subconfig.yaml").write_text(yaml.safe_dump({
+        "source": case["source"], "energy": case["energy"], "deltabeta_table": case["db"]}))
+    det = simdir.run_single_simulation(tmp_path, 0)
+    ref = bw.make_sim(case)
+    for p in range(det.shape[0]):
+        u = np.load(sub / f"u_{p:04}.npy")
+        assert u.dtype == np.complex128 and u.shape == (ref.N,)
+        assert rel_l2(bw.square_and_downsample(u, ref, ref.z_detector), det[p]) < 1e-13
+    assert not (sub / f"u_{det.shape[0]:04}.npy").exists()
