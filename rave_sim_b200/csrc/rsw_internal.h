@@ -3,6 +3,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 namespace rsw {
@@ -150,6 +151,12 @@ struct PassArgs {
     // column pass: when set, the launch functions store the kernel's resident
     // CTAs on the current device here and launch nothing
     int64_t *resident;
+    // column pass, filled in by its launch function: a 2-D TMA map over the
+    // input (rows of 2^log_n2 samples as 8-byte words; boxes of one tile's
+    // columns by up to 256 rows), through which each CTA prefetches its next
+    // tile into L2; in_map_ok 0: no prefetch
+    int in_map_ok;
+    CUtensorMap in_map;
 };
 
 // Level structure of the internal spectrum layout (log2 lengths and digit

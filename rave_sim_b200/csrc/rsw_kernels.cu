@@ -10,6 +10,40 @@
 
 namespace rsw {
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda), looked up once
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+bool encode_col_map(CUtensorMap *map, const void *in, int64_t n, int log_n2, int words_per_sample, int box_w,
+                    int box_h) {
+    const EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn || (reinterpret_cast<uintptr_t>(in) & 15) != 0 || box_w > 256 || box_h > 256) return false;
+    const int64_t row_words = (int64_t(1) << log_n2) * words_per_sample;
+    const int64_t rows = n >> log_n2;
+    if (rows < box_h || row_words < box_w || rows > (int64_t(1) << 31) || row_words > (int64_t(1) << 31))
+        return false;
+    cuuint64_t dims[2] = {cuuint64_t(row_words), cuuint64_t(rows)};
+    cuuint64_t strides[1] = {cuuint64_t(row_words * 8)};
+    cuuint32_t box[2] = {cuuint32_t(box_w), cuuint32_t(box_h)};
+    cuuint32_t elem_strides[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void *>(in), dims, strides, box, elem_strides,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 static std::atomic<unsigned long long> g_launches{0};  // host-side count of kernel launches
 void count_launch() { ++g_launches; }
 

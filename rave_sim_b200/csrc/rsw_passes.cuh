@@ -42,6 +42,14 @@ __device__ __forceinline__ double rint_d(double x) { return rint(x); }
 __device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
+// L2 prefetch of the box of a 2-D TMA map at (x, y) (x in elements of the
+// map; x times the element size a multiple of 16 bytes)
+__device__ __forceinline__ void prefetch_l2_tile(const CUtensorMap *map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y)
+                 : "memory");
+}
 
 // Range reduction of a phase to [-pi, pi] (Cody & Waite 1980, three-part
 // constant; 2pi = P1 + P2 + P3 with P1, P2 of 29 significant bits so that
@@ -752,8 +760,8 @@ __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
 // factors live in registers where the plain kernel reads them from the
 // parameter bank, so some complex128 shapes hold fewer CTAs per SM
 // (col_resident; the host then runs such sources one after the other).
-template <typename Real, int LOG_L1, int C, int E, bool DET = false, bool BATCH = false>
-__global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(PassArgs a) {
+template <typename Real, int LOG_L1, int C, int E, bool DET, bool BATCH>
+__device__ __forceinline__ void col_pass(const PassArgs &a) {
     using B = Block<Real, LOG_L1, C, E>;
     using Cx = typename B::Cx;
     // Four-step factor W_M^(n2 k1) of column n2 = col0 + c at the frequency
@@ -798,6 +806,18 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         t_end = t_first + per < tiles ? t_first + per : tiles;
         t_step = 1;
     }
+    // this CTA's next tile into L2 through the input's TMA map, one box of the
+    // tile's C columns by up to 256 rows per thread of the first few, issued
+    // right after the current tile's own loads (2^24 complex64 columns of
+    // 2^11: 124 -> 112 us per launch alone; issued before the loads it gains
+    // nothing)
+    constexpr int PF_BOX = B::L < 256 ? B::L : 256;
+    const auto prefetch_next = [&](int64_t tile) {
+        if (!a.in_map_ok || tile + t_step >= t_end || t >= B::L / PF_BOX) return;
+        const int64_t nt = tile + t_step;
+        const int x = int((nt & ((int64_t(1) << log_tb) - 1)) * C) * int(sizeof(Cx) / 8);
+        prefetch_l2_tile(&a.in_map, x, int(((nt >> log_tb) << LOG_L1) + int64_t(t) * PF_BOX));
+    };
     int parity = 0;
     for (int64_t tile = t_first; tile < t_end; tile += t_step, parity ^= 1) {
         // factor tables, double-buffered by tile parity
@@ -829,6 +849,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (flags & PF_INV) {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = gin[int64_t(B::last_pos(tp, r)) << log_n2];
+            prefetch_next(tile);
             if (flags & PF_TWI) {
                 __syncthreads();  // this tile's factor table is complete
                 const Lf *vc = vec + c * EP;
@@ -851,6 +872,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
 #pragma unroll
             for (int r = 0; r < E; ++r)
                 v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[int64_t(B::first_pos(tp, r)) << log_n2];
+            prefetch_next(tile);
         }
         // the detection variant runs the inverse only: no transmission, no forward
         // (single-transform passes transmit at base 0; a batched pass at the
@@ -890,6 +912,25 @@ __global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel
         if (!paired) __syncthreads();
     }
     if constexpr (DET) detect_finish(a.det);
+}
+
+// The column kernel. Single-source complex128 tiles of 256 threads take a
+// kernel held to two CTAs per SM: ptxas's default gave the 2^7 outer columns
+// of 2^26 three-level plans 168 registers and one CTA per SM (1028 us per
+// launch), two CTAs at 128 registers and a few spills run 774 us. (Their
+// batched variants keep the default; rsw_sim_run_batch then runs such
+// sources one by one.)
+template <typename Real, int LOG_L1, int C, int E, bool DET = false, bool BATCH = false>
+__global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT) col_pass_kernel(const __grid_constant__ PassArgs a) {
+    col_pass<Real, LOG_L1, C, E, DET, BATCH>(a);
+}
+template <typename Real, int LOG_L1, int C, int E> constexpr bool col_two_ctas() {
+    return sizeof(Real) == 8 && Block<Real, LOG_L1, C, E>::NT == 256;
+}
+template <typename Real, int LOG_L1, int C, int E, bool DET = false, bool BATCH = false>
+__global__ void __launch_bounds__(Block<Real, LOG_L1, C, E>::NT, 2)
+    col_pass_kernel_2cta(const __grid_constant__ PassArgs a) {
+    col_pass<Real, LOG_L1, C, E, DET, BATCH>(a);
 }
 
 // exp(2 pi i G N1^2 k2s^2) for every register (r, tp) of the row kernel
@@ -996,10 +1037,20 @@ constexpr int col_c(int log_l) {
 // segments, measured 26 % and 13 % faster than 32-byte ones at 2^28 and 2^24)
 constexpr int col_c64(int log_l) { return log_l == 10 ? 16 : log_l == 11 ? 8 : col_c(log_l); }
 
+// The input's TMA map for the column kernel's next-tile prefetch: rows of
+// 2^log_n2 samples of words_per_sample 8-byte words, boxes of box_w words by
+// box_h rows. False (no prefetch) when the input is not 16-byte aligned or
+// the map cannot be encoded.
+bool encode_col_map(CUtensorMap *map, const void *in, int64_t n, int log_n2, int words_per_sample, int box_w,
+                    int box_h);
+
 template <typename Real, int LG, int C, int E, bool DET = false, bool BT = false>
 static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
     using B = Block<Real, LG, C, E>;
-    auto k = col_pass_kernel<Real, LG, C, E, DET, BT>;
+    auto k = [] {
+        if constexpr (col_two_ctas<Real, LG, C, E>() && !BT) return col_pass_kernel_2cta<Real, LG, C, E, DET, BT>;
+        else return col_pass_kernel<Real, LG, C, E, DET, BT>;
+    }();
     // the per-column factor tables only when the pass applies a four-step twiddle
     const size_t plain = B::SMEM;
     const size_t tab = (B::SMEM + 15) / 16 * 16 + ColTab<B::T>::template bytes<C, E, 16>();
@@ -1021,7 +1072,11 @@ static cudaError_t col_impl(const PassArgs &a, cudaStream_t s) {
         const int64_t per = (tiles + grid - 1) / grid;
         grid = (tiles + per - 1) / per;
     }
-    k<<<dim3(unsigned(grid)), dim3(B::NT), tables ? tab : plain, s>>>(a);
+    PassArgs b = a;
+    constexpr int words = int(sizeof(typename B::Cx) / 8);
+    b.in_map_ok = a.in && !(a.flags & PF_ONES) && tiles > grid &&
+                  encode_col_map(&b.in_map, a.in, a.n, a.log_n2, words, C * words, B::L < 256 ? B::L : 256);
+    k<<<dim3(unsigned(grid)), dim3(B::NT), tables ? tab : plain, s>>>(b);
     count_launch();
     return cudaGetLastError();
 }
