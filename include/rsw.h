@@ -311,7 +311,10 @@ rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run 
  * wavelength-dependent factors, transfer function and chirp table, and the
  * detector values are added in source order, as count rsw_sim_run calls would
  * add them. The sim keeps batch buffers of count * N samples (two with phase
- * stepping), sized for the largest batch run so far. Lockstep needs a plan
+ * stepping), sized for the largest batch run so far; where they would not fit
+ * in four fifths of the device memory that is free or already held by them,
+ * the sources run in consecutive lockstep chunks that do, with the same order
+ * of accumulation. Lockstep needs a plan
  * of two or three levels, the Fresnel propagator, no history, no keypoints,
  * at least one element and a detector of at least one pixel, and no final
  * fields (rsw_sim_set_final_fields); otherwise the sources run one after the

@@ -2522,33 +2522,36 @@ static bool batch_keeps_occupancy(const rsw_plan_s *P) {
 
 extern "C" {
 
-rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
-                             void *stream) {
-    if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
-    if (count < 0 || count > RSW_BATCH_MAX)
-        return fail(RSW_ERR_INVALID, "batch of %lld sources (at most %d)", (long long)count, RSW_BATCH_MAX);
-    for (int64_t b = 0; b < count; ++b)
-        if (!(runs[b].energy_ev > 0) && !(runs[b].wavelength_m > 0))
-            return fail(RSW_ERR_INVALID, "source %lld: energy or wavelength must be positive", (long long)b);
-    rsw_plan_s *P = S->plan;
-    // lockstep needs the two- or three-level passes with the chirp form of the
-    // Fresnel kernel and the fused detection; everything else runs the
-    // sources one after the other, with the same results
-    const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
-                          S->hist_dz == 0.0 && S->keypoints.empty() && S->final_fields.empty() &&
-                          !S->els.empty() && S->geom.n_pix > 0 && batch_keeps_occupancy(P);
-    if (!lockstep) {
-        for (int64_t b = 0; b < count; ++b) CHECK(rsw_sim_run(S, src, runs + b, stream));
-        return RSW_OK;
+// Sources per lockstep chunk: as many as fit, with their batch buffers, in
+// four fifths of the device memory that is free or already held by the
+// sim's batch buffers.
+static int64_t batch_chunk(const rsw_sim_s *S, int64_t count) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return count;
     }
-    ++g_api_calls;
-    const int nb = int(count);
-    cudaStream_t st = (cudaStream_t)stream;
+    const size_t held = S->bbuf[0].bytes + S->bbuf[1].bytes;
+    const size_t per = size_t(S->d.n) * S->plan->elem() * (S->nr_phase_steps > 1 ? 2 : 1);
+    const size_t budget = (free_b + held) / 5 * 4;
+    int64_t k = std::max<int64_t>(1, std::min<int64_t>(count, per ? int64_t(budget / per) : count));
+    // RSW_BATCH_CHUNK caps the chunk (tests)
+    const int cap = env_int("RSW_BATCH_CHUNK", 0);
+    if (cap > 0) k = std::min<int64_t>(k, cap);
+    return k;
+}
+
+// One lockstep batch of nb >= 2 sources (rsw_sim_run_batch).
+static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_source_run *runs, int nb,
+                               cudaStream_t st) {
+    rsw_plan_s *P = S->plan;
     const size_t nel = S->els.size();
     const int64_t np = S->geom.n_pix;
     const int64_t stride = batch_sum_stride(np);
     if (S->batch_cap < nb) {
-        // sums and counter start at zero and are left at zero by every pass
+        // sums and counter start at zero and are left at zero by every pass;
+        // the capacity counts only once every buffer is in place
+        S->batch_cap = 0;
         const size_t fb = size_t(S->d.n) * P->elem() * size_t(nb);
         CHECK(S->bbuf[0].alloc(fb));
         if (S->nr_phase_steps > 1) CHECK(S->bbuf[1].alloc(fb));
@@ -2614,6 +2617,36 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
     CU(cudaMemcpyAsync(S->btab.p, tab.data(), tab.size() * sizeof(BatchTrans), cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(S->bweight.p, weights.data(), weights.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     return run_schedule(R, src, 0.0);
+}
+
+rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
+                             void *stream) {
+    if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
+    if (count < 0 || count > RSW_BATCH_MAX)
+        return fail(RSW_ERR_INVALID, "batch of %lld sources (at most %d)", (long long)count, RSW_BATCH_MAX);
+    for (int64_t b = 0; b < count; ++b)
+        if (!(runs[b].energy_ev > 0) && !(runs[b].wavelength_m > 0))
+            return fail(RSW_ERR_INVALID, "source %lld: energy or wavelength must be positive", (long long)b);
+    const rsw_plan_s *P = S->plan;
+    // lockstep needs the two- or three-level passes with the chirp form of the
+    // Fresnel kernel and the fused detection; everything else runs the
+    // sources one after the other, with the same results
+    const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
+                          S->hist_dz == 0.0 && S->keypoints.empty() && S->final_fields.empty() &&
+                          !S->els.empty() && S->geom.n_pix > 0 && batch_keeps_occupancy(P);
+    // consecutive chunks keep the order in which every (phase step, pixel)
+    // accumulator receives the sources
+    const int64_t chunk = lockstep ? batch_chunk(S, count) : 1;
+    for (int64_t b = 0; b < count; b += chunk) {
+        const int64_t k = std::min(chunk, count - b);
+        if (k > 1) {
+            ++g_api_calls;
+            CHECK(run_lockstep(S, src, runs + b, int(k), (cudaStream_t)stream));
+        } else {
+            CHECK(rsw_sim_run(S, src, runs + b, stream));
+        }
+    }
+    return RSW_OK;
 }
 
 }  // extern "C"

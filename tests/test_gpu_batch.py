@@ -9,7 +9,8 @@ are held to.
 
 Cases: the three-grating interferometer (gratings, phase stepping) in both
 dtypes, with each instance checked alone through one-hot weights and the
-complex64 batch checked to launch one kernel per pass for all instances; a sample
+complex64 batch checked to launch one kernel per pass for all instances; a
+batch run in chunks (RSW_BATCH_CHUNK, as when the buffers do not fit); a sample
 (int8 grid, per-energy material tables) with a cutoff angle that is active
 for some energies only; a point source; a forced three-level plan; batches
 that grow the sim's batch buffers; the configurations that run one source
@@ -180,5 +181,24 @@ def test_unbatchable_configurations_run_one_by_one():
     try:
         sim.set_history(0.2)
         assert rel_l2(_batched(sim, runs, case["source"]), _sequential(sim, runs, case["source"])) < TOL
+    finally:
+        sim.close()
+
+
+def test_batch_in_chunks(monkeypatch):
+    monkeypatch.setenv("RSW_BATCH_CHUNK", "2")
+    case = _talbot_lau("c8")
+    runs = [{"energy": e, "db_table": workloads.db_table(e), "weight": 1.0 + i} for i, e in enumerate(ENERGIES)]
+    sim = Simulation(case, dtype="c8")
+    try:
+        lib = rsw.load_library()
+        l0 = lib.rsw_launch_count()
+        seq = _sequential(sim, runs, case["source"])
+        l1 = lib.rsw_launch_count()
+        bat = _batched(sim, runs, case["source"])
+        l2 = lib.rsw_launch_count()
+        assert rel_l2(bat, seq) < TOL
+        # chunks of 2, 2 and 1 sources: three runs' worth of pass launches
+        assert (l2 - l1) * 5 < (l1 - l0) * 4
     finally:
         sim.close()
