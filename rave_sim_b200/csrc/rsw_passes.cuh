@@ -516,8 +516,9 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
         if constexpr (B::NS == 1) __syncthreads();  // no barrier inside a one-stage transform
         const Cx *__restrict__ gin = static_cast<const Cx *>(a.in) + (row << LOG_L2);
         Cx *__restrict__ gout = static_cast<Cx *>(a.out) + (row << LOG_L2);
-        {
-            // this CTA's next row into L2 while this one is transformed
+        // this CTA's next row into L2 while this one is transformed, issued
+        // after this row's own loads
+        const auto prefetch_next = [&] {
             constexpr uint32_t chunk = uint32_t(L * sizeof(Cx) / 32);
             if constexpr (chunk >= 16 && chunk % 16 == 0) {
                 if (!(flags & PF_ONES) && row + gridDim.x < rows && tp < 32)
@@ -525,11 +526,12 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
                                          tp * chunk,
                                      chunk);
             }
-        }
+        };
         Cx v[E];
         if (!(flags & PF_SPEC_IN)) {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = (flags & PF_ONES) ? one_c<Cx>() : gin[B::first_pos(tp, r)];
+            prefetch_next();
             if (TWF && (flags & PF_TWF)) {
                 __syncthreads();  // this row's factor table is complete
 #pragma unroll
@@ -557,6 +559,7 @@ __global__ void __launch_bounds__(Block<Real, LOG_L2, 1, E>::NT, row_min_ctas<Re
         } else {
 #pragma unroll
             for (int r = 0; r < E; ++r) v[r] = gin[B::last_pos(tp, r)];
+            prefetch_next();
         }
 
         if constexpr (CHIRP) {
