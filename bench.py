@@ -333,13 +333,18 @@ def main():
     tuning = {}
     if not args.no_autotune:
         # the schedule of each field length chosen by timing (registered for
-        # the simulations created below)
+        # the simulations created below), on batches of that length's fields
+        # when its sources run in lockstep (up to 4 GiB of fields)
         from rave_sim_b200 import autotune
 
-        for n_g in sorted({int(g["case"]["sim_params"]["N"]) for g in groups}):
-            r = autotune.tune(n_g, args.dtype, reps=5, save=False)
+        for g in groups:
+            n_g = int(g["case"]["sim_params"]["N"])
+            fields = 1
+            if not args.no_batch and len(g["energies"]) > 1:
+                fields = max(1, min(len(g["energies"]), (4 << 30) // (n_g * s_bytes)))
+            r = autotune.tune(n_g, args.dtype, reps=3 if fields > 1 else 5, save=False, fields=fields)
             tuning[str(n_g)] = {"choice": r["best"], "ms_per_split_step": r["ms_per_split_step"],
-                                "candidates": len(r["tried"])}
+                                "fields": fields, "candidates": len(r["tried"])}
     for g in groups:
         g["sim"] = rsw.Simulation(g["case"], grids=g["grids"], dtype=args.dtype)
         g["n"] = int(g["case"]["sim_params"]["N"])

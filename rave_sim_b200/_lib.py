@@ -117,6 +117,8 @@ SIGNATURES = {
     "rsw_set_tuning": (C.c_int, [_I64, C.c_int, C.POINTER(Tuning)]),
     "rsw_autotune": (C.c_int, [_I64, C.c_int, C.c_int, C.POINTER(Tuning), _DP, C.POINTER(Tuning), _DP,
                                C.c_int, C.POINTER(C.c_int), _P]),
+    "rsw_autotune_batch": (C.c_int, [_I64, C.c_int, _I64, C.c_int, C.POINTER(Tuning), _DP, C.POINTER(Tuning), _DP,
+                               C.c_int, C.POINTER(C.c_int), _P]),
     "rsw_plan_destroy": (C.c_int, [_P]),
     "rsw_plan_info": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                 C.POINTER(C.c_int), C.POINTER(_I64)]),

@@ -3,7 +3,8 @@ of each kernel, chosen by timing on the device (the choice cuFFT makes inside
 cufftPlan1d, fast-wave/src/fft.cpp:8, made here by measurement).
 
 ``tune(n, dtype)`` times every available tuning of a length on one
-steady-state split step (``rsw_autotune``), registers the fastest for the
+steady-state split step (``rsw_autotune``, or ``rsw_autotune_batch`` over
+several fields at once), registers the fastest for the
 plans and simulations created afterwards in this process
 (``rsw_set_tuning``) and records it in a JSON cache, keyed by device name,
 length and dtype. ``load_cache()`` registers the cached tunings of the
@@ -59,23 +60,27 @@ def plan_tuning(plan) -> dict:
     return _to_dict(t)
 
 
-def tune(n: int, dtype="c8", reps: int = 5, register_result: bool = True, save: bool = True) -> dict:
+def tune(n: int, dtype="c8", reps: int = 5, register_result: bool = True, save: bool = True,
+         fields: int = 1) -> dict:
     """Time every available tuning of (n, dtype); returns {"best": tuning,
     "ms_per_split_step": t, "tried": [(tuning, ms), ...]} and registers /
-    caches the best one."""
+    caches the best one. ``fields`` > 1 times each split step over that many
+    fields of n samples in one launch per pass, as a lockstep batch of
+    sources runs (``rsw_autotune_batch``); the times are then per split step
+    of all fields."""
     lib = L.load()
     code = dtype_code(dtype)
     best, best_ms, count = L.Tuning(), C.c_double(), C.c_int()
     cap = 256
     tried = (L.Tuning * cap)()
     tried_ms = (C.c_double * cap)()
-    L.check(lib.rsw_autotune(int(n), code, int(reps), C.byref(best), C.byref(best_ms), tried, tried_ms, cap,
-                             C.byref(count), _stream_ptr()))
+    L.check(lib.rsw_autotune_batch(int(n), code, int(fields), int(reps), C.byref(best), C.byref(best_ms), tried,
+                                   tried_ms, cap, C.byref(count), _stream_ptr()))
     out = {"best": _to_dict(best), "ms_per_split_step": best_ms.value,
            "tried": [(_to_dict(tried[i]), tried_ms[i]) for i in range(min(count.value, cap))]}
     if register_result:
         register(n, dtype, out["best"])
-    if save:
+    if save and fields == 1:  # the cache holds single-field tunings
         _save_entry(n, code, out["best"], best_ms.value)
     return out
 

@@ -996,7 +996,13 @@ rsw_status rsw_set_tuning(int64_t n, int dtype, const rsw_tuning *t) {
 // field of n samples on the device, and the fastest is returned.
 rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double *best_ms, rsw_tuning *tried,
                         double *tried_ms, int max_tried, int *n_tried, void *stream) {
+    return rsw_autotune_batch(n, dtype, 1, reps, best, best_ms, tried, tried_ms, max_tried, n_tried, stream);
+}
+
+rsw_status rsw_autotune_batch(int64_t n, int dtype, int64_t fields, int reps, rsw_tuning *best, double *best_ms,
+                              rsw_tuning *tried, double *tried_ms, int max_tried, int *n_tried, void *stream) {
     if (!best) return fail(RSW_ERR_INVALID, "best is NULL");
+    if (fields < 1 || fields > RSW_BATCH_MAX) return fail(RSW_ERR_INVALID, "fields must be in [1, %d]", RSW_BATCH_MAX);
     if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
     if (n < 16 || (n & (n - 1)) != 0)
         return fail(RSW_ERR_UNSUPPORTED, "N = %lld: this version supports powers of two >= 16", (long long)n);
@@ -1034,9 +1040,9 @@ rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double
     cudaStream_t s = (cudaStream_t)stream;
     const size_t elem = dtype == RSW_C128 ? 16 : 8;
     DevBuf field;
-    CHECK(field.alloc(size_t(n) * elem));
+    CHECK(field.alloc(size_t(n) * size_t(fields) * elem));
     {
-        cudaError_t e = launch_fill_ones(field.p, n, dtype == RSW_C128, s);
+        cudaError_t e = launch_fill_ones(field.p, n * fields, dtype == RSW_C128, s);
         if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "fill: %s", cudaGetErrorString(e));
     }
     // a grating sub-step at 46 keV on a 2 nm grid, 10 um thick, no cutoff
@@ -1070,6 +1076,7 @@ rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double
         DevBuf h3;
         if (pl->log_n1 > 0 && h3.alloc(size_t(int64_t(1) << pl->log_nr) * 16) != RSW_OK) continue;
         PassArgs a = base_args(pl.get());
+        a.n = n * fields;  // the passes over all fields, one launch each
         a.in = field.p;
         a.out = field.p;
         a.tr = tr;

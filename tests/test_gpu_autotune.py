@@ -54,3 +54,24 @@ def test_unavailable_tuning_rejected():
         rsw.Plan(1 << 20, "c16", tuning={"levels": 2, "log_rows": 10, "row_e": 8})  # rows of 2^10: no E=8
     with pytest.raises(L.RswError):
         rsw.Plan(1 << 26, "c16", tuning={"levels": 1})
+
+
+@pytest.mark.parametrize("dt", ["c16", "c8"])
+def test_batched_autotune(dt, monkeypatch):
+    # rsw_autotune_batch times every candidate over several fields in one
+    # launch per pass: the same candidates, each time the split step of all
+    # fields (longer than one field's), and the best of them registered
+    for v in ("RSW_SPLIT", "RSW_SPLIT3", "RSW_ROW_E", "RSW_COL_E"):
+        monkeypatch.delenv(v, raising=False)
+    n = 1 << 18
+    try:
+        one = autotune.tune(n, dt, reps=2, save=False, register_result=False)
+        four = autotune.tune(n, dt, reps=2, save=False, fields=4)
+        assert sorted(map(str, (t for t, _ in four["tried"]))) == sorted(map(str, (t for t, _ in one["tried"])))
+        assert four["ms_per_split_step"] == pytest.approx(min(ms for _, ms in four["tried"]))
+        assert four["ms_per_split_step"] > one["ms_per_split_step"]
+        assert autotune.plan_tuning(rsw.Plan(n, dt)) == four["best"]
+    finally:
+        autotune.register(n, dt, None)
+    with pytest.raises(L.RswError):
+        autotune.tune(n, dt, reps=1, save=False, register_result=False, fields=0)
