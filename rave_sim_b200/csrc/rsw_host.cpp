@@ -859,7 +859,7 @@ static rsw_status create_plan(rsw_plan *out, int64_t n, int dtype, const rsw_tun
     if (dtype != RSW_C128 && dtype != RSW_C64) return fail(RSW_ERR_INVALID, "unknown dtype %d", dtype);
     // lengths that are not a power of two, and powers of two below 16
     if (n >= 1 && ((n & (n - 1)) != 0 || n < 16)) return create_blue_plan(out, n, dtype);
-    int lg, l1, lb, lr;
+    int lg = 0, l1 = 0, lb = 0, lr = 0;
     CHECK(plan_split(n, dtype, &lg, &l1, &lb, &lr, t));
     std::unique_ptr<rsw_plan_s> p(new (std::nothrow) rsw_plan_s());
     if (!p) return fail(RSW_ERR_NOMEM, "host allocation failed");
