@@ -330,10 +330,14 @@ rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run 
  * at least one element and a detector of at least one pixel, and no final
  * fields (rsw_sim_set_final_fields); otherwise the sources run one after the
  * other through rsw_sim_run. A batch keeps no
- * final field (rsw_sim_final_field). count <= RSW_BATCH_MAX. */
+ * final field (rsw_sim_final_field). count <= RSW_BATCH_MAX.
+ * d_each (device memory, may be NULL) receives each source's own detector
+ * values as well, unweighted, source b's [phase][pix] at
+ * d_each + b * nr_phase_steps * n_pix: the detected.npy of one source that
+ * big-wave's run_single_simulation writes (big-wave/multisim.py:118-143). */
 #define RSW_BATCH_MAX 4096
 rsw_status rsw_sim_run_batch(rsw_sim sim, const rsw_source *src, const rsw_source_run *runs,
-                             int64_t count, void *stream);
+                             int64_t count, double *d_each, void *stream);
 /* Zero the accumulator. */
 rsw_status rsw_sim_reset(rsw_sim sim, void *stream);
 /* Copy the accumulator (nr_phase_steps * n_pix doubles) to host memory;

@@ -1718,6 +1718,9 @@ struct Runner {
     std::vector<std::vector<double>> cuts; // cutoff frequency per instance and cutoff index
     const BatchTrans *btr = nullptr;       // entries of the element being applied
     std::vector<std::pair<double, int>> prop_keys;  // (dz, cutoff index) of each transfer-function table
+    // optional: each source's own detector values (unweighted), instance b's
+    // [phase][pix] at each + b * nr_phase_steps * n_pix
+    double *each = nullptr;
 
     // chirp table for a distance dz at this run's wavelength (built on first use)
     rsw_status chirp_for(PropArgs &pr, double dz) {
@@ -1979,7 +1982,7 @@ struct Runner {
         if (!(mid && P->log_n1 > 0 && np > 0)) {
             CHECK(finalize());
             if (fin) CU(cudaMemcpyAsync(fin, bp(cur), size_t(P->n) * P->elem(), cudaMemcpyDeviceToDevice, st));
-            return detect(phase, weight);
+            return detect(phase, weight, each ? each + phase * np : nullptr);
         }
         const int dst = target();
         PassArgs a = base_args(P);
@@ -2009,6 +2012,10 @@ struct Runner {
             d.bweight = (const double *)S->bweight.p;
             d.n_inst = nb;
         }
+        if (each) {
+            d.inst_out = each + phase * np;
+            d.inst_stride = S->nr_phase_steps * np;
+        }
         TimingLog::Rec r{};
         if (S->tl.enabled) S->tl.begin(2, st, r);
         cudaError_t e = launch_col_detect(a, P->dbl(), P->col_e, st);
@@ -2022,13 +2029,14 @@ struct Runner {
         return RSW_OK;
     }
 
-    rsw_status detect(int64_t phase, double weight) {
+    // out: also the phase step's pixel values (unweighted), or NULL
+    rsw_status detect(int64_t phase, double weight, double *out = nullptr) {
         TimingLog::Rec r{};
         if (S->tl.enabled) S->tl.begin(2, st, r);
         double *acc = (double *)S->acc.p + phase * S->geom.n_pix;
         double *comp = (double *)S->comp.p + phase * S->geom.n_pix;
         cudaError_t e = launch_detect(S->buf[cur].p, (const int64_t *)S->bounds.p, (const double *)S->cosv.p,
-                                      (const double *)S->rv.p, S->geom.n_pix, S->d.dx, S->d.pixel_size_y, nullptr,
+                                      (const double *)S->rv.p, S->geom.n_pix, S->d.dx, S->d.pixel_size_y, out,
                                       acc, comp, weight, P->dbl(), st);
         if (e != cudaSuccess) return fail(RSW_ERR_CUDA, "detect: %s", cudaGetErrorString(e));
         if (S->tl.enabled) S->tl.end(r, st);
@@ -2485,7 +2493,11 @@ static rsw_status run_schedule(Runner &R, const rsw_source *src, double weight) 
 
 extern "C" {
 
-rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
+}  // extern "C"
+
+// One source (rsw_sim_run); each: also its own detector values, or NULL.
+static rsw_status run_one(rsw_sim_s *S, const rsw_source *src, const rsw_source_run *run, void *stream,
+                          double *each) {
     if (!S || !src || !run) return fail(RSW_ERR_INVALID, "NULL argument");
     if (!(run->energy_ev > 0) && !(run->wavelength_m > 0))
         return fail(RSW_ERR_INVALID, "energy or wavelength must be positive");
@@ -2495,6 +2507,7 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     R.P = S->plan;
     R.st = (cudaStream_t)stream;
     R.fbuf = S->buf;
+    R.each = each;
     R.wl = run_wavelength(run);
     R.wls.assign(1, R.wl);
     for (double a : S->cutoff_angles) R.cut.push_back(std::sin(a) / R.wl);
@@ -2504,6 +2517,12 @@ rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *r
     CU(cudaMemcpyAsync(S->mat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
     CU(cudaMemcpyAsync(S->mat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
     return run_schedule(R, src, run->weight);
+}
+
+extern "C" {
+
+rsw_status rsw_sim_run(rsw_sim S, const rsw_source *src, const rsw_source_run *run, void *stream) {
+    return run_one(S, src, run, stream, nullptr);
 }
 
 }  // extern "C"
@@ -2550,7 +2569,7 @@ static int64_t batch_chunk(const rsw_sim_s *S, int64_t count) {
 
 // One lockstep batch of nb >= 2 sources (rsw_sim_run_batch).
 static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_source_run *runs, int nb,
-                               cudaStream_t st) {
+                               cudaStream_t st, double *each) {
     rsw_plan_s *P = S->plan;
     const size_t nel = S->els.size();
     const int64_t np = S->geom.n_pix;
@@ -2577,6 +2596,7 @@ static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_so
     R.st = st;
     R.nb = nb;
     R.fbuf = S->bbuf;
+    R.each = each;
     R.cuts.resize(size_t(nb));
     std::vector<double> dbh(size_t(nb) * nel * 128 * 2, 0.0), fch(dbh.size(), 0.0);
     std::vector<BatchTrans> tab(nel * 2 * size_t(nb));
@@ -2627,7 +2647,7 @@ static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_so
 }
 
 rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
-                             void *stream) {
+                             double *d_each, void *stream) {
     if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
     if (count < 0 || count > RSW_BATCH_MAX)
         return fail(RSW_ERR_INVALID, "batch of %lld sources (at most %d)", (long long)count, RSW_BATCH_MAX);
@@ -2644,13 +2664,15 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
     // consecutive chunks keep the order in which every (phase step, pixel)
     // accumulator receives the sources
     const int64_t chunk = lockstep ? batch_chunk(S, count) : 1;
+    const int64_t per_source = S->nr_phase_steps * S->geom.n_pix;  // d_each values of one source
     for (int64_t b = 0; b < count; b += chunk) {
         const int64_t k = std::min(chunk, count - b);
+        double *each = d_each ? d_each + b * per_source : nullptr;
         if (k > 1) {
             ++g_api_calls;
-            CHECK(run_lockstep(S, src, runs + b, int(k), (cudaStream_t)stream));
+            CHECK(run_lockstep(S, src, runs + b, int(k), (cudaStream_t)stream, each));
         } else {
-            CHECK(rsw_sim_run(S, src, runs + b, stream));
+            CHECK(run_one(S, src, runs + b, stream, each));
         }
     }
     return RSW_OK;

@@ -116,6 +116,10 @@ struct DetectArgs {
     const double *bweight;
     int64_t sum_stride;
     int n_inst;
+    // optional: the pixel values of each instance (unweighted) also written
+    // to inst_out + b * inst_stride
+    double *inst_out;
+    int64_t inst_stride;
 };
 
 // Arguments of one pass. N = N1 * N2 samples; three-level plans split the

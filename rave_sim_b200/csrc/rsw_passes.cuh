@@ -726,7 +726,8 @@ __device__ __forceinline__ void detect_bin(const DetectArgs &d, double *sum, int
 // adds weight * value into the accumulator with Kahan compensation, and
 // zeroes the sums and the count for the next pass. A batched pass adds its
 // instances one after the other, in instance order: the order in which
-// separate runs of the same sources would add them.
+// separate runs of the same sources would add them. With inst_out it also
+// keeps each instance's own pixel values.
 __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
     __shared__ int last;
     __threadfence();  // this thread's atomics before the count
@@ -742,6 +743,7 @@ __device__ __forceinline__ void detect_finish(const DetectArgs &d) {
             double *sum = d.sum + b * d.sum_stride + j;
             const double s = __ldcg(sum);
             const double val = (((s * cj) * d.dx) * d.psy) / rj;
+            if (d.inst_out) d.inst_out[b * d.inst_stride + j] = val;
             const double w = d.bweight ? __ldg(d.bweight + b) : d.weight;
             const double y = __dsub_rn(__dmul_rn(w, val), comp);
             const double t = __dadd_rn(acc, y);

@@ -359,18 +359,26 @@ class Simulation:
         run = self._run(energy, db_table, weight, wavelength, keep)
         L.check(self._lib.rsw_sim_run(self._h, C.byref(src), C.byref(run), _stream_ptr()))
 
-    def run_sources(self, runs: Sequence[dict], *, source: dict, field=None):
+    def run_sources(self, runs: Sequence[dict], *, source: dict, field=None, each: bool = False):
         """Run several sources of the same geometry in lockstep
         (rsw_sim_run_batch): ``runs`` holds one dict per source with
         ``energy``, ``db_table`` and optional ``weight`` (1.0) and
         ``wavelength``; the detector values are added in list order, as
-        run_source calls in that order would add them."""
+        run_source calls in that order would add them. With ``each`` it
+        returns every source's own detector values, unweighted, as a CUDA
+        tensor (sources, nr_phase_steps, n_pix)."""
         keep = []
         src = self._source(source, field, keep)
         arr = (L.SourceRun * max(len(runs), 1))()
         for i, r in enumerate(runs):
             arr[i] = self._run(r["energy"], r["db_table"], r.get("weight", 1.0), r.get("wavelength"), keep)
-        L.check(self._lib.rsw_sim_run_batch(self._h, C.byref(src), arr, len(runs), _stream_ptr()))
+        out = None
+        if each:
+            torch = _torch()
+            out = torch.empty((len(runs), self.nr_phase_steps, self.n_pix), dtype=torch.float64, device="cuda")
+        L.check(self._lib.rsw_sim_run_batch(self._h, C.byref(src), arr, len(runs),
+                                            C.cast(_dptr(out), L._DP) if each else None, _stream_ptr()))
+        return out
 
     def _run(self, energy, db_table, weight, wavelength, keep):
         db = self.deltabeta_vector(db_table)

@@ -19,6 +19,10 @@ field at the detector of each phase step as ``NNNNNNNN/u_{step:04}.npy``
     python -m rave_sim_b200.simdir <sim_dir> -s <source_idx> [--dtype c8|c16] [--history_dz DZ]
         [--save_keypoints_path DIR]
 
+``-s`` also takes several indices (``0-31``, ``0,4,9-12``): ``run_simulations``
+runs the sources that share a point source as one lockstep batch and writes
+each one's detected.npy.
+
 With ``--history_dz`` the history of the source is written as
 ``history.npy`` (n_pix, entries), ``history_z.npy`` and ``history_x.npy``
 (big-wave/multisim.py:132-141). The field stays in GPU memory for the whole
@@ -157,19 +161,80 @@ def run_single_simulation(sim_dir, source_idx: int, scratch_dir=None, save_keypo
         sim.close()
 
 
+def run_simulations(sim_dir, source_indices, dtype: Optional[str] = None) -> dict:
+    """Run several sources of ``sim_dir`` and write each one's detected.npy,
+    as ``run_single_simulation`` per index would (fast-wave's loop over
+    ``-s k``, fast-wave/Readme.md:22-26). The sources share the directory's
+    setup, so those with the same point source run as one lockstep batch:
+    one launch per pass for all their energies, each source's detector kept
+    apart. Vector sources (their own input fields) and configs that save
+    final fields run one by one. Returns {index: detector array}."""
+    from .engine import Simulation
+
+    sim_dir = Path(sim_dir)
+    cases = {int(k): load_source(sim_dir, int(k)) for k in source_indices}
+    out = {}
+    groups: dict = {}
+    for k, c in cases.items():
+        src = c["source"]
+        if src["type"] == "point" and not c["save_final_u_vectors"]:
+            groups.setdefault(("point", src["x"], src["z"]), []).append(k)
+        else:
+            out[k] = run_single_simulation(sim_dir, k, dtype=dtype)
+    for (_, x, z), ks in groups.items():
+        c = cases[ks[0]]
+        dt = dtype or c["dtype"]
+        sim = Simulation(c, grids=c["grids"], dtype=dt, cutoff_angles=c["cutoff_angles"])
+        try:
+            sim.reset()
+            each = sim.run_sources([{"energy": cases[k]["energy"], "db_table": cases[k]["db"]} for k in ks],
+                                   source={"type": "point", "x": x, "z": z}, each=True).cpu().numpy()
+        finally:
+            sim.close()
+        for k, det in zip(ks, each):
+            np.save(sub_dir(sim_dir, k) / "detected.npy", det)
+            out[k] = det
+    return out
+
+
+def parse_indices(spec: str) -> list:
+    """Source indices of ``-s``: ``7``, ``0-31`` or ``0,4,9-12``."""
+    ks = []
+    for part in spec.split(","):
+        part = part.strip()
+        if "-" in part:
+            a, b = part.split("-", 1)
+            a, b = int(a), int(b)
+            if b < a:
+                raise ValueError(f"empty range {part!r}")
+            ks.extend(range(a, b + 1))
+        else:
+            ks.append(int(part))
+    if not ks or min(ks) < 0:
+        raise ValueError(f"bad source indices {spec!r}")
+    return ks
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m rave_sim_b200.simdir",
-                                 description="Run one source of a rave-sim simulation directory on the GPU engine.")
+                                 description="Run sources of a rave-sim simulation directory on the GPU engine.")
     ap.add_argument("sim_dir")
-    ap.add_argument("-s", "--source_idx", type=int, required=True)
+    ap.add_argument("-s", "--source_idx", required=True,
+                    help="source index, or several: 0-31, 0,4,9-12 (run together where they share a point source)")
     ap.add_argument("--dtype", choices=["c8", "c16"], default=None, help="override the config's dtype")
     ap.add_argument("--history_dz", type=float, default=None)
     ap.add_argument("--save_keypoints_path", default=None,
                     help="directory for keypoint_{element:02}_{0|1}.npy (the field before / after each element)")
     a = ap.parse_args(argv)
     try:
-        run_single_simulation(a.sim_dir, a.source_idx, save_keypoints_path=a.save_keypoints_path,
-                              history_dz=a.history_dz, dtype=a.dtype)
+        ks = parse_indices(a.source_idx)
+        if len(ks) > 1 and (a.history_dz or a.save_keypoints_path):
+            raise ValueError("--history_dz and --save_keypoints_path take a single source index")
+        if len(ks) == 1:
+            run_single_simulation(a.sim_dir, ks[0], save_keypoints_path=a.save_keypoints_path,
+                                  history_dz=a.history_dz, dtype=a.dtype)
+        else:
+            run_simulations(a.sim_dir, ks, dtype=a.dtype)
     except Exception as e:  # mirror fastwave: message and non-zero exit, no traceback
         print(f"error: {e}", file=sys.stderr)
         return 1

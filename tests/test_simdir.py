@@ -101,6 +101,21 @@ def test_cli_reports_errors_without_traceback(tmp_path, capsys):
     assert "error:" in capsys.readouterr().err
 
 
+def test_parse_source_indices():
+    assert simdir.parse_indices("7") == [7]
+    assert simdir.parse_indices("0-3") == [0, 1, 2, 3]
+    assert simdir.parse_indices("0,4,9-11") == [0, 4, 9, 10, 11]
+    for bad in ("", "3-1", "-2", "a"):
+        with pytest.raises(ValueError):
+            simdir.parse_indices(bad)
+
+
+def test_cli_several_sources_reject_history(tmp_path, capsys):
+    _write_snapshot_dir(tmp_path)
+    assert simdir.main([str(tmp_path), "-s", "0-1", "--history_dz", "0.1"]) == 1
+    assert "single source index" in capsys.readouterr().err
+
+
 def test_detector_x_vector_matches_reference_formula():
     # util.detector_x_vector (big-wave/util.py:78-82)
     x = simdir.detector_x_vector(2.5e-05, 1.0e-06)
@@ -171,3 +186,38 @@ def test_cli_history(tmp_path):
     assert h.shape == h_ref.shape
     assert rel_l2(h, h_ref) < 1e-10
     assert x.shape == (h.shape[0],)
+
+
+def _add_sources(root, energies, x=None):
+    """Further subconfigs beside 00000000: the same point source (or one at
+    x), other energies, deltabeta scaled by (E0 / E)^2."""
+    sub0 = yaml.safe_load((root / "00000000" / "subconfig.yaml").read_text())
+    e0 = float(sub0["energy"])
+    ks = []
+    for i, e in enumerate(energies, start=1):
+        sub = dict(sub0, energy=float(e))
+        r = (e0 / e) ** 2
+        sub["deltabeta_table"] = [[m, [v[0] * r, v[1] * r * r]] for m, v in sub0["deltabeta_table"]]
+        if x is not None and i == len(energies):
+            sub["source"] = dict(sub0["source"], x=float(x))
+        d = root / f"{i:08}"
+        d.mkdir()
+        (d / "subconfig.yaml").write_text(yaml.safe_dump(sub))
+        ks.append(i)
+    return [0] + ks
+
+
+@gpu
+def test_several_sources_match_one_by_one(tmp_path):
+    # sources 0-3 share the point source and run as one batch, source 4 has
+    # its own; every detected.npy equals that source's own run
+    _need_cuda()
+    _write_snapshot_dir(tmp_path)
+    ks = _add_sources(tmp_path, [40000.0, 52000.0, 58000.0, 44000.0], x=-2e-7)
+    assert simdir.main([str(tmp_path), "-s", f"0-{ks[-1]}"]) == 0
+    batched = {k: np.load(tmp_path / f"{k:08}" / "detected.npy") for k in ks}
+    for k in ks:
+        one = simdir.run_single_simulation(tmp_path, k)
+        assert batched[k].shape == one.shape and batched[k].dtype == np.float64
+        assert rel_l2(batched[k], one) < 1e-12, k
+    assert rel_l2(batched[0], batched[1]) > 1e-3  # the energies differ
