@@ -110,10 +110,12 @@ rsw_status rsw_set_tuning(int64_t n, int dtype, const rsw_tuning *tuning);
 rsw_status rsw_autotune(int64_t n, int dtype, int reps, rsw_tuning *best, double *best_ms,
                         rsw_tuning *tried, double *tried_ms, int max_tried, int *n_tried, void *stream);
 /* No counterpart in the reference: rsw_autotune with each split step timed
- * over `fields` transforms of length n in one launch per pass, the way
- * rsw_sim_run_batch runs the sources of one field length (a field buffer of
- * fields * n samples is allocated here). *best_ms and tried_ms are per split
- * step of all fields. fields = 1 is rsw_autotune. The fastest choice for a
+ * over `fields` transforms of length n in one launch per pass, the launch
+ * shape in which rsw_sim_run_batch runs the sources of one field length
+ * (the plain pass kernels over the fields; the batched kernels add only the
+ * per-source table reads). A field buffer of fields * n samples is
+ * allocated here. *best_ms and tried_ms are per split step of all fields.
+ * fields = 1 is rsw_autotune. The fastest choice for a
  * batch can differ from the fastest for one field: 2^24 complex128 in
  * batches of 32 runs 2 % faster with 16 samples per thread in both passes,
  * one field with 8. */
