@@ -315,8 +315,11 @@ rsw_status rsw_sim_shape(rsw_sim sim, int64_t *nr_phase_steps, int64_t *n_pix,
  * accumulator. Asynchronous on `stream`. */
 rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run *run,
                        void *stream);
-/* Run `count` sources (runs[0 .. count-1]: energies, deltabeta, weights) of
- * the same source geometry in lockstep. Replaces the reference's one run per
+/* Run `count` sources (runs[0 .. count-1]: energies, deltabeta, weights) in
+ * lockstep. srcs holds n_sources = 1 source description shared by all runs,
+ * or one per run (n_sources = count); sources of one lockstep batch share
+ * their type and z, and point positions and vector fields may differ (an
+ * extended source spot). Replaces the reference's one run per
  * source (big-wave/wavesim.py:84-298 called once per energy by
  * big-wave/multisim.py:50-150; fast-wave's one invocation per source index,
  * fast-wave/Readme.md:22-26): every split step of all sources is one launch
@@ -329,17 +332,18 @@ rsw_status rsw_sim_run(rsw_sim sim, const rsw_source *src, const rsw_source_run 
  * the sources run in consecutive lockstep chunks that do, with the same order
  * of accumulation. Lockstep needs a plan
  * of two or three levels, the Fresnel propagator, no history, no keypoints,
- * at least one element and a detector of at least one pixel, and no final
- * fields (rsw_sim_set_final_fields); otherwise the sources run one after the
- * other through rsw_sim_run. A batch keeps no
+ * at least one element and a detector of at least one pixel, no final
+ * fields (rsw_sim_set_final_fields) and sources of one type and z;
+ * otherwise the sources run one after the other through rsw_sim_run. A batch keeps no
  * final field (rsw_sim_final_field). count <= RSW_BATCH_MAX.
  * d_each (device memory, may be NULL) receives each source's own detector
  * values as well, unweighted, source b's [phase][pix] at
  * d_each + b * nr_phase_steps * n_pix: the detected.npy of one source that
  * big-wave's run_single_simulation writes (big-wave/multisim.py:118-143). */
 #define RSW_BATCH_MAX 4096
-rsw_status rsw_sim_run_batch(rsw_sim sim, const rsw_source *src, const rsw_source_run *runs,
-                             int64_t count, double *d_each, void *stream);
+rsw_status rsw_sim_run_batch(rsw_sim sim, const rsw_source *srcs, int64_t n_sources,
+                             const rsw_source_run *runs, int64_t count, double *d_each,
+                             void *stream);
 /* Zero the accumulator. */
 rsw_status rsw_sim_reset(rsw_sim sim, void *stream);
 /* Copy the accumulator (nr_phase_steps * n_pix doubles) to host memory;

@@ -145,7 +145,7 @@ SIGNATURES = {
     "rsw_sim_destroy": (C.c_int, [_P]),
     "rsw_sim_shape": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
     "rsw_sim_run": (C.c_int, [_P, C.POINTER(Source), C.POINTER(SourceRun), _P]),
-    "rsw_sim_run_batch": (C.c_int, [_P, C.POINTER(Source), C.POINTER(SourceRun), _I64, _DP, _P]),
+    "rsw_sim_run_batch": (C.c_int, [_P, C.POINTER(Source), _I64, C.POINTER(SourceRun), _I64, _DP, _P]),
     "rsw_sim_reset": (C.c_int, [_P, _P]),
     "rsw_sim_read": (C.c_int, [_P, _DP, _P]),
     "rsw_sim_read_device": (C.c_int, [_P, _DP, _P]),

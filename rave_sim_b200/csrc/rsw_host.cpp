@@ -2371,7 +2371,12 @@ static double run_wavelength(const rsw_source_run *run) {
 // The per-source schedule of big-wave/wavesim.py:84-298 on R's instances:
 // source, elements (phase-step snapshot before the first stepped element),
 // detector, then the remaining phase steps from the snapshot.
-static rsw_status run_schedule(Runner &R, const rsw_source *src, double weight) {
+// srcs: one source for every instance (n_srcs 1) or one per instance
+// (n_srcs R.nb), all of one type and z; point positions and vector fields
+// may differ between instances.
+static rsw_status run_schedule(Runner &R, const rsw_source *srcs, int64_t n_srcs, double weight) {
+    const rsw_source *src = srcs;  // type, z (and everything of a single source)
+    const auto src_of = [&](int b) { return n_srcs > 1 ? srcs + b : srcs; };
     rsw_sim_s &s = *R.S;
     const double z_tol = 1e-8;
     const int nel = int(s.els.size());
@@ -2389,17 +2394,18 @@ static rsw_status run_schedule(Runner &R, const rsw_source *src, double weight) 
     if (src->type == RSW_SRC_POINT) {
         // grid_density_check (big-wave/propagation.py:31-45), per instance
         const double dzs = z - src->z;
-        auto dist_x = [&](double idx) {
-            const double a = (double(s.d.n) / 2.0 - idx) * s.d.dx + std::fabs(src->x);
-            return std::sqrt(a * a + dzs * dzs);
-        };
         for (int b = 0; b < R.nb; ++b) {
+            const double xs = src_of(b)->x;
+            auto dist_x = [&](double idx) {
+                const double a = (double(s.d.n) / 2.0 - idx) * s.d.dx + std::fabs(xs);
+                return std::sqrt(a * a + dzs * dzs);
+            };
             const double wl = R.wls[size_t(b)];
             if (!(std::fabs(dist_x(0.0) - dist_x(1.0)) <= wl / 2.0))
                 return fail(RSW_ERR_INVALID, "Nyquist not satisfied, dx too large for the point source at dz = %g",
                             dzs);
             CHECK(rsw_point_source(R.P, static_cast<char *>(R.bp(0)) + size_t(b) * fbytes, s.d.dx, wl, z - src->z,
-                                   src->x, (void *)R.st));
+                                   xs, (void *)R.st));
         }
         CHECK(R.split_step(TransArgs{}, 0.0, ci));
         if (R.hist_on) {
@@ -2426,14 +2432,15 @@ static rsw_status run_schedule(Runner &R, const rsw_source *src, double weight) 
         if (src->type == RSW_SRC_PLANE) {
             R.ones = true;
             R.cur = -1;
-        } else if (src->d_field || src->h_field) {
-            // the same input field for every instance
-            const cudaMemcpyKind kind = src->d_field ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-            const void *from = src->d_field ? src->d_field : src->h_field;
-            for (int b = 0; b < R.nb; ++b)
-                CU(cudaMemcpyAsync(static_cast<char *>(R.bp(0)) + size_t(b) * fbytes, from, fbytes, kind, R.st));
         } else {
-            return fail(RSW_ERR_INVALID, "vector source without a field");
+            // each instance's input field (or the one field of all of them)
+            for (int b = 0; b < R.nb; ++b) {
+                const rsw_source *sb = src_of(b);
+                if (!sb->d_field && !sb->h_field) return fail(RSW_ERR_INVALID, "vector source without a field");
+                const cudaMemcpyKind kind = sb->d_field ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+                const void *from = sb->d_field ? sb->d_field : sb->h_field;
+                CU(cudaMemcpyAsync(static_cast<char *>(R.bp(0)) + size_t(b) * fbytes, from, fbytes, kind, R.st));
+            }
         }
         const double dz = z - src->z;
         if (dz != 0.0) CHECK(R.gap(dz, ci, src->z));
@@ -2516,7 +2523,7 @@ static rsw_status run_one(rsw_sim_s *S, const rsw_source *src, const rsw_source_
     CHECK(load_deltabeta(*S, run, R.wl, R.db, dbh.data(), fch.data()));
     CU(cudaMemcpyAsync(S->mat_db.p, dbh.data(), dbh.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
     CU(cudaMemcpyAsync(S->mat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, R.st));
-    return run_schedule(R, src, run->weight);
+    return run_schedule(R, src, 1, run->weight);
 }
 
 extern "C" {
@@ -2568,8 +2575,8 @@ static int64_t batch_chunk(const rsw_sim_s *S, int64_t count) {
 }
 
 // One lockstep batch of nb >= 2 sources (rsw_sim_run_batch).
-static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_source_run *runs, int nb,
-                               cudaStream_t st, double *each) {
+static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *srcs, int64_t n_srcs, const rsw_source_run *runs,
+                               int nb, cudaStream_t st, double *each) {
     rsw_plan_s *P = S->plan;
     const size_t nel = S->els.size();
     const int64_t np = S->geom.n_pix;
@@ -2643,14 +2650,21 @@ static rsw_status run_lockstep(rsw_sim_s *S, const rsw_source *src, const rsw_so
     CU(cudaMemcpyAsync(S->bmat_fac.p, fch.data(), fch.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(S->btab.p, tab.data(), tab.size() * sizeof(BatchTrans), cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(S->bweight.p, weights.data(), weights.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    return run_schedule(R, src, 0.0);
+    return run_schedule(R, srcs, n_srcs, 0.0);
 }
 
-rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_run *runs, int64_t count,
-                             double *d_each, void *stream) {
-    if (!S || !src || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
+rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *srcs, int64_t n_sources, const rsw_source_run *runs,
+                             int64_t count, double *d_each, void *stream) {
+    if (!S || !srcs || (!runs && count > 0)) return fail(RSW_ERR_INVALID, "NULL argument");
     if (count < 0 || count > RSW_BATCH_MAX)
         return fail(RSW_ERR_INVALID, "batch of %lld sources (at most %d)", (long long)count, RSW_BATCH_MAX);
+    if (n_sources != 1 && n_sources != count)
+        return fail(RSW_ERR_INVALID, "%lld source descriptions for %lld runs (1 or one per run)",
+                    (long long)n_sources, (long long)count);
+    const auto src_of = [&](int64_t b) { return n_sources > 1 ? srcs + b : srcs; };
+    bool same_kind = true;  // one type and z: lockstep possible
+    for (int64_t b = 1; b < n_sources; ++b)
+        same_kind = same_kind && srcs[b].type == srcs[0].type && srcs[b].z == srcs[0].z;
     for (int64_t b = 0; b < count; ++b)
         if (!(runs[b].energy_ev > 0) && !(runs[b].wavelength_m > 0))
             return fail(RSW_ERR_INVALID, "source %lld: energy or wavelength must be positive", (long long)b);
@@ -2660,7 +2674,8 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
     // sources one after the other, with the same results
     const bool lockstep = count > 1 && P->log_n1 > 0 && !P->blue && P->prop_mode == RSW_PROP_FRESNEL &&
                           S->hist_dz == 0.0 && S->keypoints.empty() && S->final_fields.empty() &&
-                          !S->els.empty() && S->geom.n_pix > 0 && batch_keeps_occupancy(P);
+                          !S->els.empty() && S->geom.n_pix > 0 && same_kind &&
+                          batch_keeps_occupancy(P);
     // consecutive chunks keep the order in which every (phase step, pixel)
     // accumulator receives the sources
     const int64_t chunk = lockstep ? batch_chunk(S, count) : 1;
@@ -2670,9 +2685,9 @@ rsw_status rsw_sim_run_batch(rsw_sim S, const rsw_source *src, const rsw_source_
         double *each = d_each ? d_each + b * per_source : nullptr;
         if (k > 1) {
             ++g_api_calls;
-            CHECK(run_lockstep(S, src, runs + b, int(k), (cudaStream_t)stream, each));
+            CHECK(run_lockstep(S, src_of(b), n_sources > 1 ? k : 1, runs + b, int(k), (cudaStream_t)stream, each));
         } else {
-            CHECK(run_one(S, src, runs + b, stream, each));
+            CHECK(run_one(S, src_of(b), runs + b, stream, each));
         }
     }
     return RSW_OK;

@@ -359,16 +359,27 @@ class Simulation:
         run = self._run(energy, db_table, weight, wavelength, keep)
         L.check(self._lib.rsw_sim_run(self._h, C.byref(src), C.byref(run), _stream_ptr()))
 
-    def run_sources(self, runs: Sequence[dict], *, source: dict, field=None, each: bool = False):
-        """Run several sources of the same geometry in lockstep
-        (rsw_sim_run_batch): ``runs`` holds one dict per source with
-        ``energy``, ``db_table`` and optional ``weight`` (1.0) and
-        ``wavelength``; the detector values are added in list order, as
-        run_source calls in that order would add them. With ``each`` it
-        returns every source's own detector values, unweighted, as a CUDA
-        tensor (sources, nr_phase_steps, n_pix)."""
+    def run_sources(self, runs: Sequence[dict], *, source: Optional[dict] = None, field=None, each: bool = False,
+                    sources: Optional[Sequence[dict]] = None):
+        """Run several sources in lockstep (rsw_sim_run_batch): ``runs``
+        holds one dict per source with ``energy``, ``db_table`` and optional
+        ``weight`` (1.0) and ``wavelength``; ``source`` (with ``field`` for a
+        vector source) is shared by all of them, or ``sources`` gives one
+        source dict per run (with ``u``: its own vector field). The detector
+        values are added in list order, as run_source calls in that order
+        would add them. With ``each`` it returns every source's own detector
+        values, unweighted, as a CUDA tensor (sources, nr_phase_steps, n_pix)."""
         keep = []
-        src = self._source(source, field, keep)
+        if sources is not None:
+            if len(sources) != len(runs):
+                raise ValueError("sources needs one entry per run")
+            srcs = (L.Source * max(len(sources), 1))()
+            for i, sd in enumerate(sources):
+                srcs[i] = self._source(sd, sd.get("u"), keep)
+            n_src = len(sources)
+        else:
+            srcs = (L.Source * 1)(self._source(source, field, keep))
+            n_src = 1
         arr = (L.SourceRun * max(len(runs), 1))()
         for i, r in enumerate(runs):
             arr[i] = self._run(r["energy"], r["db_table"], r.get("weight", 1.0), r.get("wavelength"), keep)
@@ -376,7 +387,7 @@ class Simulation:
         if each:
             torch = _torch()
             out = torch.empty((len(runs), self.nr_phase_steps, self.n_pix), dtype=torch.float64, device="cuda")
-        L.check(self._lib.rsw_sim_run_batch(self._h, C.byref(src), arr, len(runs),
+        L.check(self._lib.rsw_sim_run_batch(self._h, srcs, n_src, arr, len(runs),
                                             C.cast(_dptr(out), L._DP) if each else None, _stream_ptr()))
         return out
 

@@ -20,8 +20,8 @@ field at the detector of each phase step as ``NNNNNNNN/u_{step:04}.npy``
         [--save_keypoints_path DIR]
 
 ``-s`` also takes several indices (``0-31``, ``0,4,9-12``): ``run_simulations``
-runs the sources that share a point source as one lockstep batch and writes
-each one's detected.npy.
+runs the point sources at one z as one lockstep batch and writes each one's
+detected.npy.
 
 With ``--history_dz`` the history of the source is written as
 ``history.npy`` (n_pix, entries), ``history_z.npy`` and ``history_x.npy``
@@ -165,10 +165,11 @@ def run_simulations(sim_dir, source_indices, dtype: Optional[str] = None) -> dic
     """Run several sources of ``sim_dir`` and write each one's detected.npy,
     as ``run_single_simulation`` per index would (fast-wave's loop over
     ``-s k``, fast-wave/Readme.md:22-26). The sources share the directory's
-    setup, so those with the same point source run as one lockstep batch:
-    one launch per pass for all their energies, each source's detector kept
-    apart. Vector sources (their own input fields) and configs that save
-    final fields run one by one. Returns {index: detector array}."""
+    setup, so the point sources at one z run as one lockstep batch (their x
+    positions may differ): one launch per pass for all of them, each
+    source's detector kept apart. Vector sources (their own input files) and
+    configs that save final fields run one by one. Returns {index: detector
+    array}."""
     from .engine import Simulation
 
     sim_dir = Path(sim_dir)
@@ -178,17 +179,17 @@ def run_simulations(sim_dir, source_indices, dtype: Optional[str] = None) -> dic
     for k, c in cases.items():
         src = c["source"]
         if src["type"] == "point" and not c["save_final_u_vectors"]:
-            groups.setdefault(("point", src["x"], src["z"]), []).append(k)
+            groups.setdefault(src["z"], []).append(k)
         else:
             out[k] = run_single_simulation(sim_dir, k, dtype=dtype)
-    for (_, x, z), ks in groups.items():
+    for ks in groups.values():
         c = cases[ks[0]]
         dt = dtype or c["dtype"]
         sim = Simulation(c, grids=c["grids"], dtype=dt, cutoff_angles=c["cutoff_angles"])
         try:
             sim.reset()
             each = sim.run_sources([{"energy": cases[k]["energy"], "db_table": cases[k]["db"]} for k in ks],
-                                   source={"type": "point", "x": x, "z": z}, each=True).cpu().numpy()
+                                   sources=[cases[k]["source"] for k in ks], each=True).cpu().numpy()
         finally:
             sim.close()
         for k, det in zip(ks, each):
@@ -220,7 +221,7 @@ def main(argv=None) -> int:
                                  description="Run sources of a rave-sim simulation directory on the GPU engine.")
     ap.add_argument("sim_dir")
     ap.add_argument("-s", "--source_idx", required=True,
-                    help="source index, or several: 0-31, 0,4,9-12 (run together where they share a point source)")
+                    help="source index, or several: 0-31, 0,4,9-12 (point sources at one z run together)")
     ap.add_argument("--dtype", choices=["c8", "c16"], default=None, help="override the config's dtype")
     ap.add_argument("--history_dz", type=float, default=None)
     ap.add_argument("--save_keypoints_path", default=None,

@@ -202,3 +202,54 @@ def test_batch_in_chunks(monkeypatch):
         assert (l2 - l1) * 5 < (l1 - l0) * 4
     finally:
         sim.close()
+
+
+@pytest.mark.parametrize("dtype", ["c16", "c8"])
+def test_point_sources_at_several_x_in_one_batch(dtype):
+    # one source description per run: point sources at one z, different x
+    # (an extended source spot), against the same sources one by one
+    case = _point_case()
+    db = [[["Si", 2.34], [2.2888e-7, 2.5847e-10]], [["Au", 19.32], [1.4981e-6, 3.6174e-8]]]
+    xs = [0.1e-6, -0.3e-6, 0.45e-6, 0.0]
+    runs = [{"energy": 46000.0 + 1000.0 * i, "db_table": db, "weight": 1.0} for i in range(len(xs))]
+    srcs = [{"type": "point", "x": x, "z": 0.0} for x in xs]
+    sim = Simulation(case, dtype=dtype)
+    try:
+        lib = rsw.load_library()
+        l0 = lib.rsw_launch_count()
+        each = sim.run_sources(runs, sources=srcs, each=True).cpu().numpy()
+        l1 = lib.rsw_launch_count()
+        for r, s_, e in zip(runs, srcs, each):
+            sim.reset()
+            sim.run_source(energy=r["energy"], db_table=r["db_table"], source=s_)
+            assert rel_l2(e, sim.detected()) < TOL
+        if dtype == "c8":  # one batch, not four runs
+            l2 = lib.rsw_launch_count()
+            assert (l1 - l0) * 2 < (l2 - l1)
+        # sources at different z cannot share a batch: they run one by one
+        mixed = [dict(srcs[0]), dict(srcs[1], z=-0.01)]
+        each = sim.run_sources(runs[:2], sources=mixed, each=True).cpu().numpy()
+        for r, s_, e in zip(runs[:2], mixed, each):
+            sim.reset()
+            sim.run_source(energy=r["energy"], db_table=r["db_table"], source=s_)
+            assert rel_l2(e, sim.detected()) < TOL
+    finally:
+        sim.close()
+
+
+def test_vector_sources_with_their_own_fields():
+    case = _talbot_lau("c16")
+    n = case["sim_params"]["N"]
+    rng = np.random.default_rng(5)
+    fields = [np.exp(1j * rng.uniform(-0.1, 0.1, n)) for _ in range(3)]
+    runs = [{"energy": e, "db_table": workloads.db_table(e), "weight": 1.0} for e in ENERGIES[:3]]
+    srcs = [{"type": "vector", "z": 0.0, "u": f} for f in fields]
+    sim = Simulation(case, dtype="c16")
+    try:
+        each = sim.run_sources(runs, sources=srcs, each=True).cpu().numpy()
+        for r, f, e in zip(runs, fields, each):
+            sim.reset()
+            sim.run_source(energy=r["energy"], db_table=r["db_table"], source={"type": "vector", "z": 0.0}, field=f)
+            assert rel_l2(e, sim.detected()) < TOL
+    finally:
+        sim.close()
